@@ -1,0 +1,155 @@
+"""Lanczos ground state, adaptive Krylov exp(-iHt) and the toolkit helpers.
+
+``timeevolve`` mirrors src/algorithms/TimeEvolution.jl:556-649 (keyword names,
+defaults, forward-only errors, column order).  ``lanczos_e0`` is the new
+ground-state entry built on the same CGS2 Lanczos builder
+(TimeEvolution.jl:250-306).  ``gapratio``/``meangapratio``/``productstate``
+mirror src/ToolKit.jl:15-37, 103-109.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as E
+from .operator import Operator
+
+
+def _opts(max_steps, nev, tol, check_every, precision, refine_steps, reorth, complex_vectors):
+    o = E.LanczosOpts()
+    o.max_steps = int(max_steps)
+    o.nev = int(nev)
+    o.tol = float(tol)
+    o.check_every = int(check_every)
+    o.precision = {"fp64": E.PREC_FP64, "mixed": E.PREC_MIXED}[precision]
+    o.refine_steps = int(refine_steps)
+    o.reorth = 1 if reorth else 0
+    o.complex_vectors = 1 if complex_vectors else 0
+    return o
+
+
+def _diag_dict(d: E.LanczosDiag):
+    return {f: getattr(d, f) for f, _ in d._fields_}
+
+
+def lanczos_e0(H: Operator, v0=None, *, m=300, nev=1, tol=0.0, check_every=10,
+               precision="fp64", refine_steps=20, reorth=True, complex_vectors=False, seed=0,
+               return_coeffs=False):
+    """Lowest `nev` eigenvalues of Hermitian H by Lanczos with full CGS2
+    reorthogonalisation.  `tol` = 0 runs exactly `m` steps; otherwise the run
+    stops once the lowest Ritz values change by less than tol (relative)
+    between checks.  precision="mixed" stores the Krylov vectors in FP32 and
+    refines the ground state in FP64."""
+    D = H.size(1)
+    if v0 is None:
+        v0 = np.random.default_rng(seed).standard_normal(D)
+    dt = E.C128 if np.iscomplexobj(v0) else E.F64
+    v0 = np.ascontiguousarray(v0, dtype=np.complex128 if dt == E.C128 else np.float64)
+    o = _opts(m, nev, tol, check_every, precision, refine_steps, reorth, complex_vectors)
+    ev = np.zeros(nev)
+    a = np.zeros(m)
+    b = np.zeros(m)
+    d = E.LanczosDiag()
+    E.check(E.load().edk_lanczos_e0(H._h, C.byref(o), E.ptr(v0), dt, E.HOST, E.ptr(ev), E.ptr(a),
+                                    E.ptr(b), C.byref(d)))
+    info = _diag_dict(d)
+    if return_coeffs:
+        n = d.steps
+        return ev, info, a[:n], b[:n]
+    return ev, info
+
+
+def batch_lanczos_e0(ops, v0s=None, *, m=200, nev=1, tol=0.0, check_every=10, precision="fp64",
+                     refine_steps=20, reorth=True, seed=0):
+    """Lanczos over many independent operators (sectors / instances)."""
+    rng = np.random.default_rng(seed)
+    if v0s is None:
+        v0s = [rng.standard_normal(op.size(1)) for op in ops]
+    cx = any(np.iscomplexobj(v) for v in v0s)
+    cat = np.concatenate([np.asarray(v, np.complex128 if cx else np.float64) for v in v0s])
+    o = _opts(m, nev, tol, check_every, precision, refine_steps, reorth, False)
+    hs = (C.c_void_p * len(ops))(*[op._h.value for op in ops])
+    ev = np.zeros(len(ops) * nev)
+    d = E.LanczosDiag()
+    E.check(E.load().edk_batch_lanczos_e0(len(ops), hs, C.byref(o), E.ptr(cat),
+                                          E.C128 if cx else E.F64, E.ptr(ev), C.byref(d)))
+    return ev.reshape(len(ops), nev), _diag_dict(d)
+
+
+class KrylovEvolutionDiagnostics(dict):
+    def __getattr__(self, k):
+        return self[k]
+
+
+def timeevolve(H: Operator, psi0, t, *, return_diagnostics=False, tol=1e-10, m_init=30,
+               m_max=60, extend_step=10, nsample=13, bisect_iters=12, reuse_basis=True,
+               extend_basis=True, normalize_output=False, precision="fp64"):
+    """timeevolve(H, ψ0, t) / timeevolve(H, ψ0, ts) — TimeEvolution.jl:556-577."""
+    scalar = np.isscalar(t)
+    ts = np.atleast_1d(np.asarray(t, dtype=np.float64))
+    if scalar and ts[0] < 0:
+        raise ValueError(f"timeevolve!: requested time {t} precedes anchor time 0.0")
+    if np.any(ts < 0):
+        raise ValueError("timeevolve: all times in ts must be non-negative; backward evolution "
+                         "is not supported")
+    psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
+    D = H.size(1)
+    if psi0.shape[0] != D:
+        raise ValueError("psi0 has the wrong length")
+    o = E.KrylovOpts()
+    E.load().edk_krylov_default_opts(C.byref(o))
+    o.tol, o.m_init, o.m_max, o.extend_step = tol, m_init, m_max, extend_step
+    o.nsample, o.bisect_iters = nsample, bisect_iters
+    o.reuse_basis, o.extend_basis = int(reuse_basis), int(extend_basis)
+    o.normalize_output = int(normalize_output)
+    o.precision = {"fp64": E.PREC_FP64, "mixed": E.PREC_MIXED}[precision]
+    out = np.zeros((D, len(ts)), dtype=np.complex128, order="F")
+    d = E.KrylovDiag()
+    E.check(E.load().edk_krylov_evolve(H._h, C.byref(o), E.ptr(psi0), E.ptr(ts), len(ts),
+                                       E.ptr(out), E.HOST, C.byref(d)))
+    diag = KrylovEvolutionDiagnostics(
+        basis_builds=d.basis_builds, basis_extensions=d.basis_extensions, restarts=d.restarts,
+        matvecs=d.matvecs, total_times_served=d.total_times_served, max_dim_used=d.max_dim_used,
+        accepted_intervals=list(d.accepted_intervals[: min(d.n_intervals, 64)]),
+        seconds=d.seconds)
+    res = out[:, 0] if scalar else out
+    return (res, diag) if return_diagnostics else res
+
+
+def tridiag_eigen(a, b):
+    """eigen(SymTridiagonal(a, b)) with the library's host eigensolver."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    m = len(a)
+    bb = np.ascontiguousarray(np.asarray(b, dtype=np.float64)[: max(m - 1, 0)])
+    if len(bb) == 0:
+        bb = np.zeros(1)
+    w = np.zeros(m)
+    Q = np.zeros((m, m), order="F")
+    if E.load().edk_tridiag_eigen(m, E.ptr(a), E.ptr(bb), E.ptr(w), E.ptr(Q)) != 0:
+        raise RuntimeError("tridiagonal eigensolver did not converge")
+    return w, Q
+
+
+# ---------------------------------------------------------------------------
+# ToolKit.jl
+# ---------------------------------------------------------------------------
+def gapratio(E_):
+    """Adjacent-gap ratios of a sorted spectrum (ToolKit.jl:15-28)."""
+    dE = np.diff(np.asarray(E_, dtype=np.float64))
+    a, b = dE[:-1], dE[1:]
+    r = np.where(a < b, a / np.where(b == 0, 1, b), np.where(a > b, b / np.where(a == 0, 1, a), 1.0))
+    return r
+
+
+def meangapratio(E_):
+    """ToolKit.jl:37."""
+    return float(np.sum(gapratio(E_)) / (len(E_) - 2))
+
+
+def productstate(v, B):
+    """Unit vector at the position of digit string v in basis B (ToolKit.jl:103-109)."""
+    s = np.zeros(B.size(1))
+    _, pos = B.index(np.asarray(v, dtype=np.int64))
+    s[pos - 1] = 1.0
+    return s

@@ -1,0 +1,208 @@
+// edk_internal.cuh — device-side data layout shared by the libedk sources.
+//
+// HBM layout of one basis (sector):
+//   I     uint64[D]   sorted 0-based representative states (EDKit's I - 1)
+//   R     f64[D]      orbit norms (symmetric kinds only)
+//   htab  slots       open-addressing table state -> (row << 5 | norm class)
+//   phase c128[len]   translation phase table C (or generator phase tables)
+// Vectors are column-major blocks x[row + k*ld] of f64 / c128 / f32 / c64.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/edk.h"
+
+namespace edk {
+
+void set_error(const std::string& msg);
+const std::string& get_error();
+
+#define EDK_TRY_CUDA(call)                                                          \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) {                                                        \
+      edk::set_error(std::string(#call) + " failed: " + cudaGetErrorString(e_));    \
+      return (e_ == cudaErrorMemoryAllocation) ? EDK_OOM : EDK_CUDA_ERROR;          \
+    }                                                                               \
+  } while (0)
+
+#define EDK_CHECK_ARG(cond, msg)                 \
+  do {                                           \
+    if (!(cond)) {                               \
+      edk::set_error(msg);                       \
+      return EDK_INVALID_ARG;                    \
+    }                                            \
+  } while (0)
+
+#define EDK_RETURN_IF(st) \
+  do {                    \
+    edk_status s_ = (st); \
+    if (s_ != EDK_OK) return s_; \
+  } while (0)
+
+// Owning device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  edk_status alloc(size_t n) {
+    release();
+    if (n == 0) return EDK_OK;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      set_error(std::string("cudaMalloc(") + std::to_string(n) + " bytes) failed: " +
+                cudaGetErrorString(e));
+      return EDK_OOM;
+    }
+    bytes = n;
+    return EDK_OK;
+  }
+  template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// ---------------------------------------------------------------------------
+// lookup / canonicalisation kinds (compile-time dispatch)
+// ---------------------------------------------------------------------------
+enum LookupKind : int {
+  BK_TENSOR = 0,     // row = state
+  BK_PROJ_RANK = 1,  // row = colex rank among fixed-popcount states
+  BK_PROJ_HASH = 2,  // row = hash(state)
+  BK_TRANS0 = 3,     // translation, trivial phase (k = 0): min over rotations
+  BK_TRANS = 4,      // translation, phase C[M] from the first-minimum shift M
+  BK_TRANSPAR = 5,   // translation + reflection
+  BK_ABELIAN = 6     // generic odometer over commuting generators
+};
+
+constexpr int kMaxGen = 8;
+constexpr int kMaxLayers = 64;
+constexpr int kNormClasses = 32;
+constexpr uint32_t kHashEmpty32 = 0xFFFFFFFFu;
+
+enum GenKind : int { GEN_PERM = 0, GEN_ROTL = 1, GEN_REV = 2, GEN_ID = 3 };
+
+struct GenDev {
+  int kind;      // GenKind
+  int order;     // cyclic order
+  int shift;     // rotation amount for GEN_ROTL
+  int nlayers;   // delta-swap layers for GEN_PERM
+  uint64_t inv_mask;
+  int phase_off; // offset into the phase table
+  int pad;
+  uint64_t lmask[kMaxLayers];
+  int lshift[kMaxLayers];
+};
+
+// Everything a kernel needs to know about a basis; passed by value.
+struct BasisDev {
+  int bk;          // LookupKind
+  int L, A, len;   // sites, unit cell, number of translations
+  int64_t D;
+  uint64_t maskL;  // (1 << L) - 1
+  const uint64_t* I;     // states (nullptr for TensorBasis)
+  const double* R;       // norms (nullptr for onsite kinds)
+  // hash table (BK_PROJ_HASH / translation kinds / abelian)
+  const void* htab;
+  uint64_t hmask;        // slots - 1
+  int packed;            // 1: value = row << 5 | class; 0: value = row, R gathered
+  int nclass;
+  double Rcls[kNormClasses];
+  // BK_PROJ_RANK
+  int K;                 // popcount of every state
+  // phases
+  const double2* phase;  // translation: len entries; abelian: concatenated tables
+  int P;                 // parity sign (TranslationParityBasis)
+  int phase_real;        // 1 when every phase is real
+  // abelian generators
+  int ngen;
+  const GenDev* gens;
+};
+
+// Local terms compiled for the device.
+// Family: 2-site terms (i, i+d mod L) sharing one 4x4 matrix, evaluated on
+// whole bit planes: X = s, Y = rotl(s, d), local column c = 2*X_p + Y_p.
+struct FamDev {
+  int d;
+  int nnz[4];         // off-diagonal entries per local column
+  uint64_t valid;     // bit p set when the family has a term with site i at bit p
+  double2 dval[4];    // diagonal values M[c][c]
+  int xr[4][3];       // c ^ r for each off-diagonal entry (bit1: site i, bit0: site j)
+  double2 val[4][3];  // M[r][c]
+};
+// Generic term on up to 8 sites (bit positions, most significant site first).
+struct TermDev {
+  int nsites;
+  int bitpos[8];
+  int col_off;        // offset into colptr (2^nsites + 1 entries)
+  int diag_off;       // offset into dval (2^nsites entries)
+};
+struct OpDev {
+  int nfam;
+  const FamDev* fam;
+  int nterm;
+  const TermDev* term;
+  const int* colptr;        // per term: start of the off-diagonal list of each column
+  const uint64_t* xmask;    // XOR mask turning the row state into the column state
+  const double2* val;       // matrix element M[r][c]
+  const double2* dval;      // diagonal M[c][c]
+};
+
+}  // namespace edk
+
+// Opaque handles of the C ABI.
+struct edk_basis {
+  edk_basis_desc desc{};
+  int kind = 0;
+  int L = 0, A = 1, len = 1, K = -1, P = 1, Kmom = 0;  // Kmom = mod(-k, len)
+  int64_t D = 0;
+  edk::DevBuf I, R, htab, phase, gens;
+  edk::BasisDev dev{};
+  std::vector<edk::GenDev> gens_host;
+  std::vector<int> gen_order, gen_q;
+  std::vector<std::vector<int>> gen_perm;
+  std::vector<std::vector<uint8_t>> gen_inv;
+  bool phase_complex = false;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  ~edk_basis();
+};
+
+struct edk_operator {
+  edk_basis* b = nullptr;
+  edk::DevBuf fam, term, colptr, xmask, val, dval;
+  edk::OpDev dev{};
+  bool gather = true;
+  bool is_complex = false;
+  int max_hits = 0;
+  int nfam = 0, ngeneric = 0;
+  // host copy of the merged terms (used by the invariance check)
+  std::vector<std::vector<int>> sites;
+  std::vector<std::vector<double>> dense_re, dense_im;  // local matrices, row-major
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  ~edk_operator();
+};
+
+namespace edk {
+// implemented in edk_apply.cu
+edk_status apply_device(edk_operator* op, int dtype, const void* x, void* y, int64_t nvec,
+                        int64_t ldx, int64_t ldy, int accumulate, cudaStream_t st);
+// implemented in edk_util.cpp
+int tridiag_eigvals(int m, const double* a, const double* b, double* w);
+int tridiag_eigen(int m, const double* a, const double* b, double* w, double* Q);
+double elapsed_ms(cudaEvent_t a, cudaEvent_t b);
+}  // namespace edk

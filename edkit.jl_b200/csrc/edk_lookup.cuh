@@ -1,0 +1,224 @@
+// edk_lookup.cuh — device-side index(b, dgt): orbit canonicalisation on
+// bit-packed states followed by a table lookup.
+//
+// The canonicalisation restates, on integers, the loops of
+//   TranslationalBasis index        src/Basis/TranslationalBasis.jl:310-341
+//   TranslationParityBasis index    src/Basis/TranslationalParityBasis.jl:192-234
+//   AbelianBasis shift_canonical    src/Basis/AbelianBasis.jl:428-445, 669-693
+// with the same first-minimum tie rule (strict <, scan order 0,1,2,...), so the
+// shift M, and hence the phase, is the reference's.  Instead of the
+// reference's binary_search over the sorted I (ProjectedBasis.jl:71-81) the row
+// is found with one open-addressing probe sequence (a state present in I maps
+// to its position in I, an absent state reports "not found" exactly where
+// binary_search returns 0).
+#pragma once
+
+#include "edk_internal.cuh"
+
+namespace edk {
+
+template <class S> struct StateBits;
+template <> struct StateBits<uint32_t> { static constexpr int bits = 32; };
+template <> struct StateBits<uint64_t> { static constexpr int bits = 64; };
+
+template <class S>
+__device__ __forceinline__ S rotr_L(S s, int a, int L, S mask) {
+  return (S)(((s >> a) | (s << (L - a))) & mask);
+}
+template <class S>
+__device__ __forceinline__ S rotl_L(S s, int a, int L, S mask) {
+  return (S)(((s << a) | (s >> (L - a))) & mask);
+}
+__device__ __forceinline__ uint32_t rev_L(uint32_t s, int L) { return __brev(s) >> (32 - L); }
+__device__ __forceinline__ uint64_t rev_L(uint64_t s, int L) { return __brevll(s) >> (64 - L); }
+__device__ __forceinline__ int popc_s(uint32_t s) { return __popc(s); }
+__device__ __forceinline__ int popc_s(uint64_t s) { return __popcll(s); }
+__device__ __forceinline__ int ffs_s(uint32_t s) { return __ffs(s) - 1; }
+__device__ __forceinline__ int ffs_s(uint64_t s) { return __ffsll((long long)s) - 1; }
+
+__host__ __device__ __forceinline__ uint32_t hmix32(uint32_t h) {
+  h ^= h >> 16; h *= 0x85ebca6bu; h ^= h >> 13; h *= 0xc2b2ae35u; h ^= h >> 16;
+  return h;
+}
+__host__ __device__ __forceinline__ uint64_t hmix64(uint64_t h) {
+  h ^= h >> 33; h *= 0xff51afd7ed558ccdull; h ^= h >> 33; h *= 0xc4ceb9fe1a85ec53ull;
+  h ^= h >> 33;
+  return h;
+}
+
+// 32-bit keys: one 8-byte slot = key << 32 | value, empty = all ones.
+__device__ __forceinline__ bool hash_find(const BasisDev& b, uint32_t key, uint32_t& val) {
+  const unsigned long long* tab = reinterpret_cast<const unsigned long long*>(b.htab);
+  uint64_t slot = hmix32(key) & b.hmask;
+  for (uint64_t n = 0; n <= b.hmask; ++n) {
+    unsigned long long e = __ldg(tab + slot);
+    if (e == ~0ull) return false;
+    if ((uint32_t)(e >> 32) == key) { val = (uint32_t)e; return true; }
+    slot = (slot + 1) & b.hmask;
+  }
+  return false;
+}
+// 64-bit keys: 16-byte slots {key, value}, empty key = all ones.
+__device__ __forceinline__ bool hash_find(const BasisDev& b, uint64_t key, uint32_t& val) {
+  const ulonglong2* tab = reinterpret_cast<const ulonglong2*>(b.htab);
+  uint64_t slot = hmix64(key) & b.hmask;
+  for (uint64_t n = 0; n <= b.hmask; ++n) {
+    ulonglong2 e = __ldg(tab + slot);
+    if (e.x == ~0ull) return false;
+    if (e.x == key) { val = (uint32_t)e.y; return true; }
+    slot = (slot + 1) & b.hmask;
+  }
+  return false;
+}
+
+// decode a hash value into (row, norm)
+__device__ __forceinline__ void decode_val(const BasisDev& b, uint32_t v, int64_t& pos,
+                                           double& rpos) {
+  if (b.packed) {
+    pos = (int64_t)(v >> 5);
+    rpos = b.Rcls[v & 31u];
+  } else {
+    pos = (int64_t)v;
+    rpos = __ldg(b.R + pos);
+  }
+}
+
+// colex rank of a fixed-popcount state (= its position among all states with
+// that popcount in ascending order); binom[p*33 + k] = C(p, k), p < 32.
+__device__ __forceinline__ int64_t colex_rank(uint32_t s, const uint32_t* binom) {
+  uint32_t r = 0;
+  int j = 1;
+  while (s) {
+    int p = __ffs(s) - 1;
+    r += binom[p * 33 + j];
+    s &= s - 1;
+    ++j;
+  }
+  return (int64_t)r;
+}
+__device__ __forceinline__ int64_t colex_rank(uint64_t s, const uint32_t* binom) {
+  return colex_rank((uint32_t)s, binom);  // rank mode is only enabled for L <= 32
+}
+
+// One odometer step over the generators — AbelianBasis.jl:292-299 / 405-414.
+template <class S>
+__device__ __forceinline__ S apply_gen(const GenDev& g, S s, int L, S mask) {
+  switch (g.kind) {
+    case GEN_ROTL: s = rotl_L(s, g.shift, L, mask); break;
+    case GEN_REV: s = rev_L(s, L); break;
+    case GEN_ID: break;
+    default:
+      for (int q = 0; q < g.nlayers; ++q) {
+        S lm = (S)g.lmask[q];
+        int sh = g.lshift[q];
+        S delta = ((s >> sh) ^ s) & lm;
+        s = s ^ delta ^ (S)(delta << sh);
+      }
+  }
+  return (S)(s ^ (S)g.inv_mask);
+}
+
+// Result of index(b, state) on the device.
+struct Hit {
+  int64_t pos;   // 0-based row
+  double pre, pim;  // phase of the state relative to its representative
+  double rpos;   // norm R[pos]
+};
+
+// index(b, s): returns false where EDKit returns (0, 1).
+template <int BK, class S>
+__device__ __forceinline__ bool lookup(const BasisDev& b, S s, const uint32_t* binom, Hit& h) {
+  h.pre = 1.0; h.pim = 0.0; h.rpos = 1.0;
+  const S mask = (S)b.maskL;
+  if constexpr (BK == BK_TENSOR) {
+    h.pos = (int64_t)s;
+    return true;
+  } else if constexpr (BK == BK_PROJ_RANK) {
+    if (popc_s(s) != b.K) return false;
+    h.pos = colex_rank(s, binom);
+    return true;
+  } else if constexpr (BK == BK_PROJ_HASH) {
+    uint32_t v;
+    if (!hash_find(b, s, v)) return false;
+    h.pos = b.packed ? (int64_t)(v >> 5) : (int64_t)v;
+    return true;
+  } else if constexpr (BK == BK_TRANS0) {
+    // trivial phase: the representative is the minimum over all rotations
+    S m = s, t = s;
+    for (int i = 1; i < b.len; ++i) {
+      t = rotr_L(t, b.A, b.L, mask);
+      m = t < m ? t : m;
+    }
+    uint32_t v;
+    if (!hash_find(b, m, v)) return false;
+    decode_val(b, v, h.pos, h.rpos);
+    return true;
+  } else if constexpr (BK == BK_TRANS) {
+    // TranslationalBasis.jl:318-325: rotate right by A, stop on return,
+    // keep the first strict minimum and its shift M.
+    S I0 = s, Im = s, t = s;
+    int M = 0;
+    for (int i = 1; i < b.len; ++i) {
+      t = rotr_L(t, b.A, b.L, mask);
+      if (t == I0) break;
+      if (t < Im) { Im = t; M = i; }
+    }
+    uint32_t v;
+    if (!hash_find(b, Im, v)) return false;
+    decode_val(b, v, h.pos, h.rpos);
+    double2 c = __ldg(b.phase + M);
+    h.pre = c.x; h.pim = c.y;
+    return true;
+  } else if constexpr (BK == BK_TRANSPAR) {
+    // TranslationalParityBasis.jl:204-231
+    S Ia0 = s, t = s;
+    S Iam = Ia0, Ibm = rev_L(s, b.L);
+    int Rr = 0, M = 0;
+    for (int i = 1; i < b.len; ++i) {
+      t = rotr_L(t, b.A, b.L, mask);
+      if (t == Ia0) break;
+      if (t < Iam) { Iam = t; Rr = i; }
+      S tb = rev_L(t, b.L);
+      if (tb < Ibm) { Ibm = tb; M = i; }
+    }
+    S key;
+    double n;
+    if (Ibm < Iam) { key = Ibm; n = (double)b.P * __ldg(b.phase + M).x; }
+    else { key = Iam; n = __ldg(b.phase + Rr).x; }
+    uint32_t v;
+    if (!hash_find(b, key, v)) return false;
+    decode_val(b, v, h.pos, h.rpos);
+    h.pre = n;
+    return true;
+  } else {  // BK_ABELIAN: shift_canonical_int, AbelianBasis.jl:428-445
+    int cnt[kMaxGen], best[kMaxGen];
+#pragma unroll
+    for (int g = 0; g < kMaxGen; ++g) { cnt[g] = 0; best[g] = 0; }
+    int64_t order = 1;
+    for (int g = 0; g < b.ngen; ++g) order *= b.gens[g].order;
+    S cur = s, bst = s;
+    for (int64_t t = 0; t < order; ++t) {
+      for (int g = 0; g < b.ngen; ++g) {
+        cur = apply_gen(b.gens[g], cur, b.L, mask);
+        if (++cnt[g] >= b.gens[g].order) cnt[g] = 0; else break;
+      }
+      if (cur < bst) {
+        bst = cur;
+        for (int g = 0; g < b.ngen; ++g) best[g] = cnt[g];
+      }
+    }
+    uint32_t v;
+    if (!hash_find(b, bst, v)) return false;
+    decode_val(b, v, h.pos, h.rpos);
+    double pr = 1.0, pi = 0.0;
+    for (int g = 0; g < b.ngen; ++g) {
+      double2 c = __ldg(b.phase + b.gens[g].phase_off + best[g]);
+      double nr = pr * c.x - pi * c.y, ni = pr * c.y + pi * c.x;
+      pr = nr; pi = ni;
+    }
+    h.pre = pr; h.pim = pi;
+    return true;
+  }
+}
+
+}  // namespace edk

@@ -1,0 +1,234 @@
+/*
+ * edk.h — C ABI of libedk, the B200 (sm_100a) implementation of EDKit.jl's
+ * matrix-free operator application and the Lanczos / Krylov loops built on it.
+ *
+ * A Julia host binds these with `ccall` (see the binding in INTEGRATION.md);
+ * Python binds them with ctypes.  No CUDA or torch types cross this boundary:
+ * only plain pointers, sizes and the POD structs below.
+ *
+ * Conventions (identical to EDKit.jl):
+ *   - digit strings are big-endian: site 1 is the most significant digit
+ *     (src/Basis/AbstractBasis.jl:285-298); spin-1/2 digit 0 is Sz=+1/2;
+ *   - basis tables cross the boundary as Julia holds them: `I` 1-based int64,
+ *     `R` float64 norms;
+ *   - vectors are Julia column-major blocks: element (row r, column k) sits at
+ *     x[r + k*ldx]; complex numbers are interleaved {re, im};
+ *   - every function returns an edk_status; edk_last_error() gives the
+ *     message of the last failure on the calling thread.
+ *
+ * Host pointers are borrowed for the duration of a call.  Handles own their
+ * device memory and are released by the matching *_destroy function.
+ */
+#ifndef EDK_H
+#define EDK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  EDK_OK = 0,
+  EDK_INVALID_ARG = 1,
+  EDK_NOT_HERMITIAN = 2,
+  EDK_OOM = 3,
+  EDK_CUDA_ERROR = 4,
+  EDK_TIMEOUT = 5,
+  EDK_NOT_CONVERGED = 6,
+  EDK_UNSUPPORTED = 7,
+  EDK_ZERO_NORM = 8,
+  EDK_BACKWARD_TIME = 9
+} edk_status;
+
+/* element type of vectors crossing the boundary */
+typedef enum { EDK_F64 = 0, EDK_C128 = 1, EDK_F32 = 2, EDK_C64 = 3 } edk_dtype;
+
+/* where the vector pointers of a call live */
+typedef enum { EDK_HOST = 0, EDK_DEVICE = 1 } edk_ptr_kind;
+
+typedef enum {
+  EDK_TENSOR = 0,        /* TensorBasis            src/Basis/AbstractBasis.jl:217-247 */
+  EDK_PROJECTED = 1,     /* ProjectedBasis         src/Basis/ProjectedBasis.jl:14-260 */
+  EDK_TRANSLATIONAL = 2, /* TranslationalBasis     src/Basis/TranslationalBasis.jl:22-349 */
+  EDK_TRANSPARITY = 3,   /* TranslationParityBasis src/Basis/TranslationalParityBasis.jl:15-241 */
+  EDK_ABELIAN = 4        /* AbelianBasis / basis() src/Basis/AbelianBasis.jl:498-847 */
+} edk_basis_kind;
+
+typedef struct edk_basis edk_basis;
+typedef struct edk_operator edk_operator;
+
+/*
+ * Basis description.  Mirrors the keyword arguments of the Julia constructors.
+ * When `I` is NULL the library builds the tables on the device (base 2, with
+ * or without a charge N; a predicate `f` arrives as the `allow` bitmap the
+ * host evaluated).  Alternatively the host passes the tables it already holds
+ * (b.I, b.R) and the library uploads them unchanged.
+ */
+typedef struct {
+  int32_t kind;   /* edk_basis_kind */
+  int32_t L;      /* number of sites */
+  int32_t base;   /* local dimension; the GPU path supports 2 */
+  int32_t a;      /* unit cell (translational kinds), 1 otherwise */
+  int32_t k;      /* momentum label exactly as passed to the Julia constructor */
+  int32_t p;      /* parity +-1 (TranslationParityBasis) */
+  int32_t N;      /* charge in EDKit's convention (sum(dgt) == L*(base-1)-N), -1 = nothing;
+                     for EDK_ABELIAN it is basis()'s N (set bits on the Gosper path) */
+  /* EDK_ABELIAN generators, in the order basis() pushes them */
+  int32_t ngen;
+  const int32_t* gen_order; /* cyclic order of each generator */
+  const int32_t* gen_q;     /* quantum number of each generator */
+  const int32_t* gen_perm;  /* ngen x L site permutations, 1-based: site i -> perm[i] */
+  const uint8_t* gen_inv;   /* ngen x L spin-inversion flags */
+  /* optional predicate result f(dgt) as a bitmap over 0-based states
+     (bit s of word s/64); states whose bit is clear are rejected before the
+     symmetry check, exactly where the judges test F(dgt) first
+     (TranslationalBasis.jl:96, TranslationalParityBasis.jl:70) */
+  const uint64_t* allow;
+  /* optional tables, as the Julia basis holds them */
+  int64_t D;         /* number of rows in I/R */
+  const int64_t* I;  /* 1-based, ascending */
+  const double* R;   /* norms (ignored for onsite kinds) */
+} edk_basis_desc;
+
+/* Build a basis (tables on the device).  Replaces the constructors
+ * TensorBasis (AbstractBasis.jl:234), ProjectedBasis (ProjectedBasis.jl:244),
+ * TranslationalBasis (TranslationalBasis.jl:235), TranslationParityBasis
+ * (TranslationalParityBasis.jl:141) and basis() (AbelianBasis.jl:771). */
+edk_status edk_basis_create(const edk_basis_desc* desc, edk_basis** out);
+edk_status edk_basis_destroy(edk_basis* b);
+/* size(b, 1) — AbstractBasis.jl:142-146 */
+edk_status edk_basis_dim(const edk_basis* b, int64_t* D);
+/* copy the tables back (I 1-based, R norms; R is all ones for onsite kinds).
+ * Used for the bit-exact table check against b.I / b.R. */
+edk_status edk_basis_export(const edk_basis* b, int64_t* I, double* R);
+/* Batched index(b, dgt) — AbstractBasis.jl:246, ProjectedBasis.jl:52-57,
+ * TranslationalBasis.jl:310-341, TranslationalParityBasis.jl:192-234,
+ * AbelianBasis.jl:669-693.  `states` are 0-based integer states (index(dgt)-1);
+ * pos receives the 1-based position (0 when the state is not in the basis,
+ * where EDKit returns (0, 1)), coeff the interleaved complex coefficient. */
+edk_status edk_basis_index(const edk_basis* b, int64_t n, const uint64_t* states,
+                           int64_t* pos, double* coeff, int32_t ptr_kind);
+
+/* Build an operator from merged local terms — operator() Operator.jl:56-78
+ * after its site-list merge, trans_inv_operator() Operator.jl:102-108.
+ * Term t acts on nsites[t] sites (1-based, concatenated in `sites`) with a
+ * local (base^nsites)^2 matrix in Julia CSC form: colptr (1-based,
+ * base^nsites+1 entries per term), rowval (1-based), nzval (interleaved
+ * complex), nnz[t] nonzeros each, all concatenated.  The library checks each
+ * term for Hermiticity and the operator for invariance under the basis
+ * symmetries; when both hold it applies the row-gather form, otherwise the
+ * column-scatter form with atomics. */
+edk_status edk_operator_create(edk_basis* b, int32_t nterms, const int32_t* nsites,
+                               const int32_t* sites, const int64_t* nnz, const int64_t* colptr,
+                               const int64_t* rowval, const double* nzval, edk_operator** out);
+edk_status edk_operator_destroy(edk_operator* op);
+/* properties: is_hermitian_gather (1 = row-gather form), is_complex (1 = complex
+ * matrix elements), n_families (2-site term families on the bit-plane path),
+ * n_generic (remaining terms) */
+edk_status edk_operator_info(const edk_operator* op, int32_t* gather, int32_t* is_complex,
+                             int32_t* n_families, int32_t* n_generic);
+
+/* y (+)= H x for an nvec-column block — mul!(y, H, x) Operator.jl:309-328
+ * (accumulate=1) and H * x Operator.jl:372-394 (accumulate=0).  Synchronous:
+ * returns when y is written (host or device). */
+edk_status edk_apply(edk_operator* op, int32_t dtype, const void* x, void* y, int64_t nvec,
+                     int64_t ldx, int64_t ldy, int32_t accumulate, int32_t ptr_kind);
+/* Same with device pointers on a caller stream (cudaStream_t passed as void*);
+ * does not synchronise, so it can be captured into a CUDA graph. */
+edk_status edk_apply_async(edk_operator* op, int32_t dtype, const void* x, void* y,
+                           int64_t nvec, int64_t ldx, int64_t ldy, int32_t accumulate,
+                           void* stream);
+
+/* Lanczos ground state.  Extends the CGS2 builder _lanczos_build!
+ * (TimeEvolution.jl:250-306) with a tridiagonal eigensolve; replaces the
+ * dense eigvals(Hermitian(H)) path of Operator.jl:287-292 for large D. */
+typedef enum {
+  EDK_PREC_FP64 = 0,  /* vectors and products in FP64 */
+  EDK_PREC_MIXED = 1  /* FP32 vectors + FP32 products, FP64 alpha/beta/reorth
+                         accumulation and tridiagonal solve, then FP64 refinement */
+} edk_precision;
+
+typedef struct {
+  int32_t max_steps;     /* Lanczos steps (m) */
+  int32_t nev;           /* number of lowest eigenvalues wanted */
+  double tol;            /* relative stop tolerance on the Ritz values; 0 = run max_steps */
+  int32_t check_every;   /* steps between convergence checks */
+  int32_t precision;     /* edk_precision */
+  int32_t refine_steps;  /* FP64 refinement steps for EDK_PREC_MIXED */
+  int32_t reorth;        /* 1 = full CGS2 reorthogonalisation (reference), 0 = none */
+  int32_t complex_vectors; /* 1 = complex Krylov vectors even when H is real */
+} edk_lanczos_opts;
+
+typedef struct {
+  int32_t steps;         /* Lanczos steps taken (last stage) */
+  int32_t steps_low;     /* FP32 steps before refinement (mixed) */
+  int32_t matvecs;
+  int32_t breakdown;     /* 1 if the lucky-breakdown rule fired */
+  double seconds;        /* wall time inside the call, device work included */
+  double seconds_matvec; /* time in matvec kernels (CUDA events) */
+  double seconds_reorth; /* time in orthogonalisation kernels (CUDA events) */
+  double residual;       /* |beta_m * y_m| of the lowest Ritz pair */
+} edk_lanczos_diag;
+
+/* v0: starting vector (dtype v0_dtype, host or device); evals: nev values.
+ * alpha/beta (optional, may be NULL): the last stage's recurrence
+ * coefficients, max_steps entries each. */
+edk_status edk_lanczos_e0(edk_operator* op, const edk_lanczos_opts* opts, const void* v0,
+                          int32_t v0_dtype, int32_t ptr_kind, double* evals, double* alpha,
+                          double* beta, edk_lanczos_diag* diag);
+
+/* Adaptive Krylov exp(-iHt) psi — timeevolve (TimeEvolution.jl:563-577)
+ * with the cache/controller of TimeEvolution.jl:166-520.  psi0 and out are
+ * complex (EDK_C128 interleaved; out is N x nts column-major).  ts may be
+ * unsorted; columns come back in the caller's order. */
+typedef struct {
+  double tol;            /* default 1e-10 */
+  int32_t m_init;        /* default 30 */
+  int32_t m_max;         /* default 60 */
+  int32_t extend_step;   /* default 10 */
+  int32_t nsample;       /* default 13 */
+  int32_t bisect_iters;  /* default 12 */
+  int32_t reuse_basis;   /* default 1 */
+  int32_t extend_basis;  /* default 1 */
+  int32_t normalize_output; /* default 0 */
+  int32_t precision;     /* edk_precision: FP64 or mixed (FP32 Krylov vectors) */
+} edk_krylov_opts;
+
+typedef struct {
+  int32_t basis_builds, basis_extensions, restarts, matvecs, total_times_served, max_dim_used;
+  int32_t n_intervals;
+  double accepted_intervals[64]; /* first 64 accepted interval lengths */
+  double seconds;
+} edk_krylov_diag;
+
+/* Fill *opts with the reference defaults (TimeEvolution.jl:166-176). */
+void edk_krylov_default_opts(edk_krylov_opts* opts);
+edk_status edk_krylov_evolve(edk_operator* op, const edk_krylov_opts* opts, const void* psi0,
+                             const double* ts, int64_t nts, void* out, int32_t ptr_kind,
+                             edk_krylov_diag* diag);
+
+/* Batched Lanczos over independent operators (momentum sectors of one chain,
+ * or disorder instances): all matvecs of one step run as ONE kernel launch
+ * over a tile queue, the whole step is captured in a CUDA graph.  v0s holds
+ * the concatenated starting vectors (F64 or C128 per v0_dtype, host).
+ * evals receives nops x opts->nev values. */
+edk_status edk_batch_lanczos_e0(int32_t nops, edk_operator* const* ops,
+                                const edk_lanczos_opts* opts, const void* v0s, int32_t v0_dtype,
+                                double* evals, edk_lanczos_diag* diag);
+
+/* Symmetric tridiagonal eigensolver used by the Lanczos/Krylov drivers
+ * (eigen(SymTridiagonal(a, b)), TimeEvolution.jl:311-323): diagonal a[m],
+ * off-diagonal b[m-1]; w receives ascending eigenvalues, Q (may be NULL) the
+ * eigenvectors column-major m x m.  Returns 0 on success. */
+int edk_tridiag_eigen(int m, const double* a, const double* b, double* w, double* Q);
+
+/* last error message of the calling thread ("" if none) */
+const char* edk_last_error(void);
+/* library version string */
+const char* edk_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EDK_H */
