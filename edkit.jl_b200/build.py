@@ -20,7 +20,7 @@ ROOT = os.path.dirname(HERE)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
-                  "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
+                  "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"), "-I", BUILD]
 
 
 def _nvcc():
@@ -48,17 +48,39 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def source_hash() -> str:
+    """Digest of every source and header the library is built from."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in sorted(sources() + _headers()):
+        h.update(os.path.basename(f).encode())
+        with open(f, "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def _write_hash_header():
+    path = os.path.join(BUILD, "edk_srchash.h")
+    text = f'#define EDK_SRC_HASH "{source_hash()}"\n'
+    if not os.path.exists(path) or open(path).read() != text:
+        with open(path, "w") as fh:
+            fh.write(text)
+    return path
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     """Compile and link; returns the path of libedk.so."""
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     hdrs = _headers()
+    hash_h = _write_hash_header()
     jobs = []
     objs = []
     for src in sources():
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         objs.append(obj)
-        if force or _stale(obj, [src] + hdrs):
+        deps = [src] + hdrs + ([hash_h] if src.endswith("edk_util.cpp") else [])
+        if force or _stale(obj, deps):
             cmd = [nvcc] + NVFLAGS + ["-c", src, "-o", obj]
             if src.endswith(".cpp"):
                 cmd = [nvcc] + NVFLAGS + ["-x", "cu", "-c", src, "-o", obj]

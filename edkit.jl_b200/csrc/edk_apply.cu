@@ -250,6 +250,7 @@ edk_status apply_device(edk_operator* op, int dtype, const void* x, void* y, int
                         int64_t ldx, int64_t ldy, int accumulate, cudaStream_t st) {
   const BasisDev& b = op->b->dev;
   if (nvec <= 0 || b.D == 0) return EDK_OK;
+  EDK_RETURN_IF(check_basis_dev(b));
   if (!op->gather && !accumulate) {
     // column scatter accumulates with atomics: start from zero
     size_t es = dtype_size(dtype);
@@ -613,9 +614,11 @@ extern "C" edk_status edk_apply(edk_operator* op, int32_t dtype, const void* x, 
   EDK_CHECK_ARG(ptr_kind == EDK_HOST, "edk_apply: bad ptr_kind");
   if (nvec == 0 || D == 0) return EDK_OK;
   size_t es = dtype_size(dtype);
-  DevBuf dx, dy;
-  EDK_RETURN_IF(dx.alloc(D * nvec * es));
-  EDK_RETURN_IF(dy.alloc(D * nvec * es));
+  DevBuf& dx = op->hx;
+  DevBuf& dy = op->hy;
+  size_t need = (size_t)D * nvec * es;
+  if (dx.bytes < need) EDK_RETURN_IF(dx.alloc(need));
+  if (dy.bytes < need) EDK_RETURN_IF(dy.alloc(need));
   EDK_TRY_CUDA(cudaMemcpy2DAsync(dx.p, D * es, x, ldx * es, D * es, nvec, cudaMemcpyHostToDevice, st));
   if (accumulate)
     EDK_TRY_CUDA(cudaMemcpy2DAsync(dy.p, D * es, y, ldy * es, D * es, nvec, cudaMemcpyHostToDevice, st));

@@ -747,6 +747,12 @@ extern "C" edk_status edk_basis_create(const edk_basis_desc* desc, edk_basis** o
         dv.K = K;
       }
       dv.bk = rank ? BK_PROJ_RANK : BK_PROJ_HASH;
+      if (!rank && !b->htab.p) {
+        // GPU-built projected tables without the complete-sector structure
+        // (predicate bases) are looked up through the hash table
+        std::vector<double> one(1, 1.0);
+        EDK_RETURN_IF(finish_lookup_from_R(b, one, st));
+      }
     } else if (b->kind == EDK_TRANSLATIONAL) {
       dv.bk = (b->Kmom == 0) ? BK_TRANS0 : BK_TRANS;
     } else if (b->kind == EDK_TRANSPARITY) {
@@ -762,6 +768,35 @@ extern "C" edk_status edk_basis_create(const edk_basis_desc* desc, edk_basis** o
   *out = guard.release();
   return EDK_OK;
 }
+
+namespace edk {
+// Host-side guard run before every kernel launch that reads the basis tables:
+// a lookup kind is only launched with the tables it dereferences.
+edk_status check_basis_dev(const BasisDev& b) {
+  bool ok = true;
+  switch (b.bk) {
+    case BK_TENSOR: break;
+    case BK_PROJ_RANK: ok = b.I != nullptr && b.L <= 32; break;
+    case BK_PROJ_HASH: ok = b.I != nullptr && b.htab != nullptr; break;
+    case BK_TRANS0:
+    case BK_TRANS:
+    case BK_TRANSPAR:
+      ok = b.I != nullptr && b.R != nullptr && b.htab != nullptr && b.phase != nullptr &&
+           b.len >= 1 && b.len <= 64;
+      break;
+    case BK_ABELIAN:
+      ok = b.I != nullptr && b.R != nullptr && b.htab != nullptr && b.phase != nullptr &&
+           b.gens != nullptr && b.ngen >= 1 && b.ngen <= kMaxGen;
+      break;
+    default: ok = false;
+  }
+  if (b.D > 0 && !ok) {
+    set_error("internal: basis tables missing for its lookup kind");
+    return EDK_INVALID_ARG;
+  }
+  return EDK_OK;
+}
+}  // namespace edk
 
 extern "C" edk_status edk_basis_destroy(edk_basis* b) {
   delete b;
@@ -824,6 +859,7 @@ extern "C" edk_status edk_basis_index(const edk_basis* bc, int64_t n, const uint
     s_d = ds.as<uint64_t>(); p_d = dp.as<int64_t>(); c_d = dc.as<double2>();
   }
   const BasisDev& dv = b->dev;
+  EDK_RETURN_IF(check_basis_dev(dv));
   bool wide = dv.L > 32;
   int g = grid_for(n);
 #define EDK_IDX(BK)                                                                 \

@@ -184,6 +184,7 @@ struct edk_basis {
 struct edk_operator {
   edk_basis* b = nullptr;
   edk::DevBuf fam, term, colptr, xmask, val, dval;
+  edk::DevBuf hx, hy;  // staging buffers of edk_apply's host-pointer path (grow only)
   edk::OpDev dev{};
   bool gather = true;
   bool is_complex = false;
@@ -198,6 +199,8 @@ struct edk_operator {
 };
 
 namespace edk {
+// implemented in edk_basis.cu
+edk_status check_basis_dev(const BasisDev& b);
 // implemented in edk_apply.cu
 edk_status apply_device(edk_operator* op, int dtype, const void* x, void* y, int64_t nvec,
                         int64_t ldx, int64_t ldy, int accumulate, cudaStream_t st);

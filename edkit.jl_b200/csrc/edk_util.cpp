@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "edk_internal.cuh"
+#include "edk_srchash.h"
 
 namespace edk {
 
@@ -112,7 +113,7 @@ int tridiag_eigen(int m, const double* a, const double* b, double* w, double* Q)
 }  // namespace edk
 
 extern "C" const char* edk_last_error(void) { return edk::get_error().c_str(); }
-extern "C" const char* edk_version(void) { return "edk-b200 0.1.0 (sm_100a)"; }
+extern "C" const char* edk_version(void) { return "edk-b200 0.1.0 (sm_100a) src " EDK_SRC_HASH; }
 
 // exported for tests of the host eigensolver
 extern "C" int edk_tridiag_eigen(int m, const double* a, const double* b, double* w, double* Q) {

@@ -71,6 +71,7 @@ def lib():
         L.orc_operator_free.argtypes = [vp]
         L.orc_mul.argtypes = [vp, vp, vp, i64, i32]
         L.orc_mul_serial.argtypes = [vp, vp, vp, i64]
+        L.orc_mul_cols.argtypes = [vp, vp, vp, i64, i64, i64, i32]
         L.orc_dense.argtypes = [vp, vp]
         L.orc_gosper_next.restype = C.c_uint64
         L.orc_gosper_next.argtypes = [C.c_uint64]
@@ -353,6 +354,13 @@ class OOperator:
         Y = np.zeros_like(X, order="F")
         lib().orc_mul(self.h, _ptr(X), _ptr(Y), X.shape[1], int(nthreads))
         return Y[:, 0] if vec else Y
+
+    def mul_cols(self, x, j0, j1, nthreads=0):
+        """Partial mul(opt, v) over input columns j0..j1 (1-based, inclusive)."""
+        X = np.asfortranarray(np.asarray(x).reshape(self.dim, -1).astype(np.complex128))
+        Y = np.zeros_like(X, order="F")
+        lib().orc_mul_cols(self.h, _ptr(X), _ptr(Y), X.shape[1], int(j0), int(j1), int(nthreads))
+        return Y
 
     def mul_serial(self, x, y=None):
         """mul!(y, opt, x): single-threaded, accumulates into y."""

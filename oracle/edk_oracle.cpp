@@ -750,6 +750,41 @@ void orc_mul(const orc_operator* op, const double* x, double* y, int64_t nvec, i
   }
 }
 
+// mul(opt, v) restricted to the input columns j0..j1 (1-based, inclusive):
+// the same thread-private scatter as orc_mul, for bounded timing samples.
+// y (D x nvec) is overwritten with the partial product.
+void orc_mul_cols(const orc_operator* op, const double* x, double* y, int64_t nvec, int64_t j0,
+                  int64_t j1, int nthreads) {
+  const OBasis& b = *op->b;
+  int64_t D = b.dim();
+  int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+  const cplx* X = reinterpret_cast<const cplx*>(x);
+  cplx* Y = reinterpret_cast<cplx*>(y);
+  std::vector<std::vector<cplx>> Ms(nt);
+  int64_t n = j1 - j0 + 1;
+#pragma omp parallel num_threads(nt)
+  {
+    int t = omp_get_thread_num();
+    Ms[t].assign((size_t)D * nvec, cplx(0.0, 0.0));
+    int64_t each = n / nt, left = n % nt;
+    int64_t start = j0 + t * each + std::min<int64_t>(t, left);
+    int64_t stop = start + each + (t < left ? 1 : 0) - 1;
+    std::vector<int64_t> dgt(b.L);
+    std::vector<cplx> cin(nvec), cw(nvec);
+    for (int64_t j = start; j <= stop; ++j) {
+      for (int64_t k = 0; k < nvec; ++k) cin[k] = X[(j - 1) + k * D];
+      colmn(Ms[t].data(), D, nvec, *op, j, dgt.data(), cin.data(), cw.data());
+    }
+  }
+  int64_t tot = D * nvec;
+#pragma omp parallel for num_threads(nt) schedule(static)
+  for (int64_t i = 0; i < tot; ++i) {
+    cplx s = Ms[0][i];
+    for (int t = 1; t < nt; ++t) s += Ms[t][i];
+    Y[i] = s;
+  }
+}
+
 // Array(opt) — Operator.jl:171-196: dense column-major D x D complex matrix
 void orc_dense(const orc_operator* op, double* M) {
   const OBasis& b = *op->b;

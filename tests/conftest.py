@@ -22,6 +22,16 @@ def O():
 
 @pytest.fixture(scope="session")
 def ek():
-    """The product package (edkit.jl_b200/ imported as edkit_b200)."""
+    """The product package (edkit.jl_b200/ imported as edkit_b200).  Fails if
+    libedk.so was built from sources other than the ones in the tree."""
+    import importlib.util
     import __graft_entry__ as ge
-    return ge.load_package()
+    mod = ge.load_package()
+    spec = importlib.util.spec_from_file_location(
+        "edk_build", os.path.join(ROOT, "edkit.jl_b200", "build.py"))
+    bld = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bld)
+    want = bld.source_hash()
+    have = mod.version().rsplit(" ", 1)[-1]
+    assert have == want, f"libedk.so is stale (built from {have}, sources are {want})"
+    return mod
