@@ -12,6 +12,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <complex>
 #include <map>
@@ -213,13 +214,13 @@ __global__ void k_cls_from_R(const double* R, int64_t D, BasisDev b, uint8_t* cl
 }
 
 __global__ void k_hash_insert32(const uint64_t* I, const uint8_t* cls, int64_t D, int packed,
-                                unsigned long long* tab, uint64_t hmask) {
+                                unsigned long long* tab, uint64_t hmask, int hbits) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < D;
        i += (int64_t)gridDim.x * blockDim.x) {
     uint32_t key = (uint32_t)I[i];
     uint32_t val = packed ? (uint32_t)((i << 5) | (cls ? cls[i] : 0)) : (uint32_t)i;
     unsigned long long e = ((unsigned long long)key << 32) | val;
-    uint64_t slot = hmix32(key) & hmask;
+    uint64_t slot = hslot32(key, hbits);
     for (uint64_t n = 0; n <= hmask; ++n) {
       unsigned long long old = atomicCAS(tab + slot, ~0ull, e);
       if (old == ~0ull) break;
@@ -365,6 +366,13 @@ static edk_status build_hash(edk_basis* b, const uint8_t* cls_dev, cudaStream_t 
   EDK_TRY_CUDA(cudaMemsetAsync(b->htab.p, 0xFF, slots * slot_bytes, st));
   b->dev.htab = b->htab.p;
   b->dev.hmask = slots - 1;
+  int hbits = 0;
+  while ((1ull << hbits) < slots) ++hbits;
+  b->dev.hbits = hbits;
+  if (!wide && hbits > 32) {
+    set_error("edk_basis_create: lookup table beyond 2^32 slots");
+    return EDK_UNSUPPORTED;
+  }
   if (D == 0) return EDK_OK;
   if (wide)
     k_hash_insert64<<<grid_for(D), 256, 0, st>>>(b->I.as<uint64_t>(), cls_dev, D, b->dev.packed,
@@ -372,7 +380,8 @@ static edk_status build_hash(edk_basis* b, const uint8_t* cls_dev, cudaStream_t 
   else
     k_hash_insert32<<<grid_for(D), 256, 0, st>>>(b->I.as<uint64_t>(), cls_dev, D,
                                                   b->dev.packed,
-                                                  b->htab.as<unsigned long long>(), slots - 1);
+                                                  b->htab.as<unsigned long long>(), slots - 1,
+                                                  hbits);
   EDK_TRY_CUDA(cudaGetLastError());
   return EDK_OK;
 }
@@ -755,6 +764,8 @@ extern "C" edk_status edk_basis_create(const edk_basis_desc* desc, edk_basis** o
       }
     } else if (b->kind == EDK_TRANSLATIONAL) {
       dv.bk = (b->Kmom == 0) ? BK_TRANS0 : BK_TRANS;
+      const char* e = std::getenv("EDK_CANON_RUNS");
+      dv.runs_canon = (dv.bk == BK_TRANS0 && b->A == 1 && b->L <= 32 && e && e[0] == '1') ? 1 : 0;
     } else if (b->kind == EDK_TRANSPARITY) {
       dv.bk = BK_TRANSPAR;
     } else {

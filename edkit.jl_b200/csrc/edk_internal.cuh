@@ -118,6 +118,7 @@ struct BasisDev {
   // hash table (BK_PROJ_HASH / translation kinds / abelian)
   const void* htab;
   uint64_t hmask;        // slots - 1
+  int hbits;             // log2(slots)
   int packed;            // 1: value = row << 5 | class; 0: value = row, R gathered
   int nclass;
   double Rcls[kNormClasses];
@@ -127,6 +128,7 @@ struct BasisDev {
   const double2* phase;  // translation: len entries; abelian: concatenated tables
   int P;                 // parity sign (TranslationParityBasis)
   int phase_real;        // 1 when every phase is real
+  int runs_canon;        // 1: canonicalise from zero-run tops (unit cell 1, phase-free)
   // abelian generators
   int ngen;
   const GenDev* gens;
@@ -188,6 +190,9 @@ struct edk_operator {
   edk::OpDev dev{};
   bool gather = true;
   bool is_complex = false;
+  bool ff_ok = false;     // flip-flop bond-family fast path applies
+  bool use_ff = true;     // callers may switch the fast path off (A/B checks)
+  std::vector<unsigned char> ff_params;
   int max_hits = 0;
   int nfam = 0, ngeneric = 0;
   // host copy of the merged terms (used by the invariance check)

@@ -36,8 +36,10 @@ __device__ __forceinline__ int popc_s(uint64_t s) { return __popcll(s); }
 __device__ __forceinline__ int ffs_s(uint32_t s) { return __ffs(s) - 1; }
 __device__ __forceinline__ int ffs_s(uint64_t s) { return __ffsll((long long)s) - 1; }
 
+// 32-bit key mix; callers take the TOP bits (hslot32), which the two
+// multiplications mix best.
 __host__ __device__ __forceinline__ uint32_t hmix32(uint32_t h) {
-  h ^= h >> 16; h *= 0x85ebca6bu; h ^= h >> 13; h *= 0xc2b2ae35u; h ^= h >> 16;
+  h *= 0x9e3779b1u; h ^= h >> 15; h *= 0x85ebca77u;
   return h;
 }
 __host__ __device__ __forceinline__ uint64_t hmix64(uint64_t h) {
@@ -46,10 +48,15 @@ __host__ __device__ __forceinline__ uint64_t hmix64(uint64_t h) {
   return h;
 }
 
+// first slot of a 32-bit key in a table of hmask + 1 = 2^hbits slots
+__host__ __device__ __forceinline__ uint64_t hslot32(uint32_t key, int hbits) {
+  return hbits == 0 ? 0 : (uint64_t)(hmix32(key) >> (32 - hbits));
+}
+
 // 32-bit keys: one 8-byte slot = key << 32 | value, empty = all ones.
 __device__ __forceinline__ bool hash_find(const BasisDev& b, uint32_t key, uint32_t& val) {
   const unsigned long long* tab = reinterpret_cast<const unsigned long long*>(b.htab);
-  uint64_t slot = hmix32(key) & b.hmask;
+  uint64_t slot = hslot32(key, b.hbits);
   for (uint64_t n = 0; n <= b.hmask; ++n) {
     unsigned long long e = __ldg(tab + slot);
     if (e == ~0ull) return false;
@@ -118,6 +125,130 @@ __device__ __forceinline__ S apply_gen(const GenDev& g, S s, int L, S mask) {
   return (S)(s ^ (S)g.inv_mask);
 }
 
+// ---------------------------------------------------------------------------
+// 32-bit canonicalisation (L <= 32).  The state is doubled into a 64-bit word
+// w = s | s << L, so the rotation right by i is one funnel shift of (hi:lo)
+// plus a mask: three instructions per candidate rotation, no branches.  Only
+// the first strict minimum is kept, so M (the shift, hence the phase) is the
+// one the reference's loop reports; its early exit on returning to the start
+// state only skips rotations that repeat earlier ones.
+// ---------------------------------------------------------------------------
+struct Dbl32 { uint32_t lo, hi; };
+__device__ __forceinline__ Dbl32 dbl32(uint32_t s, int L) {
+  uint64_t w = (uint64_t)s | ((uint64_t)s << L);
+  return {(uint32_t)w, (uint32_t)(w >> 32)};
+}
+__device__ __forceinline__ uint32_t rotr_dbl(Dbl32 d, int i, uint32_t mask) {
+  return __funnelshift_r(d.lo, d.hi, i) & mask;
+}
+// Left-aligned doubling: V = (s | s << L) << (32 - L).  The 32-bit window
+// funnelshift_r(V, i) holds the rotation right by i in its top L bits; its
+// low 32 - L bits are other digits of the ring, which only matter when two
+// rotations tie on the top L bits (then the states are equal).
+__device__ __forceinline__ Dbl32 dbl32_top(uint32_t s, int L) {
+  uint64_t w = ((uint64_t)s | ((uint64_t)s << L)) << (32 - L);
+  return {(uint32_t)w, (uint32_t)(w >> 32)};
+}
+// min over translations by multiples of A (phase-free sectors): two
+// instructions per rotation (funnel shift + min)
+__device__ __forceinline__ uint32_t canon_min32(uint32_t s, int L, int A, int len, uint32_t mask) {
+  const Dbl32 d = dbl32_top(s, L);
+  uint32_t m = d.lo;
+  int i = A;
+#pragma unroll 4
+  for (int q = 1; q < len; ++q) {
+    m = min(m, __funnelshift_r(d.lo, d.hi, i));
+    i += A;
+  }
+  (void)mask;
+  return m >> (32 - L);
+}
+// Unit cell 1 only: the minimum rotation starts at the top of a run of zeros
+// (a 0 digit whose left neighbour is 1), so only those rotations are
+// compared: one per domain-wall pair instead of one per site.  For the top
+// q of such a run the rotation is the right shift by q + 1 = ffs position.
+__device__ __forceinline__ uint32_t canon_runs32(uint32_t s, int L, uint32_t mask) {
+  const Dbl32 d = dbl32_top(s, L);
+  uint32_t m = d.lo;
+  uint32_t z = ~s & (((s >> 1) | (s << (L - 1))) & mask);
+  while (z) {
+    const int i = __ffs(z);
+    z &= z - 1;
+    m = min(m, __funnelshift_r(d.lo, d.hi, i));
+  }
+  return m >> (32 - L);
+}
+
+// first minimum and its translation count M
+__device__ __forceinline__ uint32_t canon_arg32(uint32_t s, int L, int A, int len, uint32_t mask,
+                                                int& M) {
+  if (L <= 27) {
+    // the spare low bits carry q, so min() keeps the smallest q on ties
+    const Dbl32 d = dbl32_top(s, L);
+    const uint32_t hi_mask = ~((1u << (32 - L)) - 1u);
+    uint32_t m = d.lo & hi_mask;
+    int i = A;
+#pragma unroll 4
+    for (int q = 1; q < len; ++q) {
+      m = min(m, (__funnelshift_r(d.lo, d.hi, i) & hi_mask) | (uint32_t)q);
+      i += A;
+    }
+    M = (int)(m & ~hi_mask);
+    return m >> (32 - L);
+  }
+  const Dbl32 d = dbl32(s, L);
+  uint32_t m = s;
+  M = 0;
+  int i = A;
+#pragma unroll 4
+  for (int q = 1; q < len; ++q) {
+    const uint32_t r = rotr_dbl(d, i, mask);
+    const bool lt = r < m;
+    m = lt ? r : m;
+    M = lt ? q : M;
+    i += A;
+  }
+  return m;
+}
+// translations and reflected translations (TranslationParityBasis):
+// rev(rotr(s, i)) = rotl(rev(s), i) = rotr(rev(s), L - i).
+__device__ __forceinline__ void canon_par32(uint32_t s, int L, int A, int len, uint32_t mask,
+                                            uint32_t& Iam, int& Rr, uint32_t& Ibm, int& M) {
+  const uint32_t rs = __brev(s) >> (32 - L);
+  if (L <= 27) {
+    const Dbl32 d = dbl32_top(s, L), dr = dbl32_top(rs, L);
+    const uint32_t hi_mask = ~((1u << (32 - L)) - 1u);
+    uint32_t ma = d.lo & hi_mask, mb = dr.lo & hi_mask;
+    int i = A;
+#pragma unroll 2
+    for (int q = 1; q < len; ++q) {
+      ma = min(ma, (__funnelshift_r(d.lo, d.hi, i) & hi_mask) | (uint32_t)q);
+      mb = min(mb, (__funnelshift_r(dr.lo, dr.hi, L - i) & hi_mask) | (uint32_t)q);
+      i += A;
+    }
+    Rr = (int)(ma & ~hi_mask);
+    M = (int)(mb & ~hi_mask);
+    Iam = ma >> (32 - L);
+    Ibm = mb >> (32 - L);
+    return;
+  }
+  const Dbl32 d = dbl32(s, L);
+  const Dbl32 dr = dbl32(rs, L);
+  Iam = s; Rr = 0; Ibm = rs; M = 0;
+  int i = A;
+#pragma unroll 2
+  for (int q = 1; q < len; ++q) {
+    const uint32_t t = rotr_dbl(d, i, mask);
+    const uint32_t tb = rotr_dbl(dr, L - i, mask);
+    const bool lt = t < Iam, lb = tb < Ibm;
+    Iam = lt ? t : Iam;
+    Rr = lt ? q : Rr;
+    Ibm = lb ? tb : Ibm;
+    M = lb ? q : M;
+    i += A;
+  }
+}
+
 // Result of index(b, state) on the device.
 struct Hit {
   int64_t pos;   // 0-based row
@@ -144,10 +275,15 @@ __device__ __forceinline__ bool lookup(const BasisDev& b, S s, const uint32_t* b
     return true;
   } else if constexpr (BK == BK_TRANS0) {
     // trivial phase: the representative is the minimum over all rotations
-    S m = s, t = s;
-    for (int i = 1; i < b.len; ++i) {
-      t = rotr_L(t, b.A, b.L, mask);
-      m = t < m ? t : m;
+    S m = s;
+    if constexpr (sizeof(S) == 4) {
+      m = canon_min32(s, b.L, b.A, b.len, mask);
+    } else {
+      S t = s;
+      for (int i = 1; i < b.len; ++i) {
+        t = rotr_L(t, b.A, b.L, mask);
+        m = t < m ? t : m;
+      }
     }
     uint32_t v;
     if (!hash_find(b, m, v)) return false;
@@ -156,12 +292,17 @@ __device__ __forceinline__ bool lookup(const BasisDev& b, S s, const uint32_t* b
   } else if constexpr (BK == BK_TRANS) {
     // TranslationalBasis.jl:318-325: rotate right by A, stop on return,
     // keep the first strict minimum and its shift M.
-    S I0 = s, Im = s, t = s;
+    S Im = s;
     int M = 0;
-    for (int i = 1; i < b.len; ++i) {
-      t = rotr_L(t, b.A, b.L, mask);
-      if (t == I0) break;
-      if (t < Im) { Im = t; M = i; }
+    if constexpr (sizeof(S) == 4) {
+      Im = canon_arg32(s, b.L, b.A, b.len, mask, M);
+    } else {
+      S I0 = s, t = s;
+      for (int i = 1; i < b.len; ++i) {
+        t = rotr_L(t, b.A, b.L, mask);
+        if (t == I0) break;
+        if (t < Im) { Im = t; M = i; }
+      }
     }
     uint32_t v;
     if (!hash_find(b, Im, v)) return false;
@@ -171,15 +312,22 @@ __device__ __forceinline__ bool lookup(const BasisDev& b, S s, const uint32_t* b
     return true;
   } else if constexpr (BK == BK_TRANSPAR) {
     // TranslationalParityBasis.jl:204-231
-    S Ia0 = s, t = s;
-    S Iam = Ia0, Ibm = rev_L(s, b.L);
+    S Iam, Ibm;
     int Rr = 0, M = 0;
-    for (int i = 1; i < b.len; ++i) {
-      t = rotr_L(t, b.A, b.L, mask);
-      if (t == Ia0) break;
-      if (t < Iam) { Iam = t; Rr = i; }
-      S tb = rev_L(t, b.L);
-      if (tb < Ibm) { Ibm = tb; M = i; }
+    if constexpr (sizeof(S) == 4) {
+      uint32_t a_, b_;
+      canon_par32(s, b.L, b.A, b.len, mask, a_, Rr, b_, M);
+      Iam = a_; Ibm = b_;
+    } else {
+      S Ia0 = s, t = s;
+      Iam = Ia0; Ibm = rev_L(s, b.L);
+      for (int i = 1; i < b.len; ++i) {
+        t = rotr_L(t, b.A, b.L, mask);
+        if (t == Ia0) break;
+        if (t < Iam) { Iam = t; Rr = i; }
+        S tb = rev_L(t, b.L);
+        if (tb < Ibm) { Ibm = tb; M = i; }
+      }
     }
     S key;
     double n;
