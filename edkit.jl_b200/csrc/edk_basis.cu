@@ -609,6 +609,7 @@ extern "C" edk_status edk_basis_create(const edk_basis_desc* desc, edk_basis** o
   b->desc.gen_order = b->desc.gen_q = b->desc.gen_perm = nullptr;
   b->desc.gen_inv = nullptr;
   b->desc.allow = nullptr;
+  EDK_TRY_CUDA(cudaGetDevice(&b->device));
   EDK_TRY_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
   cudaStream_t st = b->stream;
   BasisDev& dv = b->dev;
@@ -849,6 +850,35 @@ extern "C" edk_status edk_basis_export(const edk_basis* bc, int64_t* I, double* 
   }
   return EDK_OK;
 }
+
+namespace edk {
+// launch index() for n device-resident states on stream st (no allocation);
+// used by edk_basis_index_noalloc
+edk_status index_device(const BasisDev& dv, int64_t n, const uint64_t* s_d, int64_t* p_d,
+                        double2* c_d, cudaStream_t st) {
+  EDK_RETURN_IF(check_basis_dev(dv));
+  if (n <= 0) return EDK_OK;
+  bool wide = dv.L > 32;
+  int g = grid_for(n);
+#define EDK_IDX(BK)                                                                 \
+  case BK:                                                                          \
+    if (wide) k_index<BK, uint64_t><<<g, 256, 0, st>>>(dv, n, s_d, p_d, c_d);       \
+    else k_index<BK, uint32_t><<<g, 256, 0, st>>>(dv, n, s_d, p_d, c_d);            \
+    break;
+  switch (dv.bk) {
+    EDK_IDX(BK_TENSOR)
+    EDK_IDX(BK_PROJ_RANK)
+    EDK_IDX(BK_PROJ_HASH)
+    EDK_IDX(BK_TRANS0)
+    EDK_IDX(BK_TRANS)
+    EDK_IDX(BK_TRANSPAR)
+    EDK_IDX(BK_ABELIAN)
+  }
+#undef EDK_IDX
+  EDK_TRY_CUDA(cudaGetLastError());
+  return EDK_OK;
+}
+}  // namespace edk
 
 extern "C" edk_status edk_basis_index(const edk_basis* bc, int64_t n, const uint64_t* states,
                                       int64_t* pos, double* coeff, int32_t ptr_kind) {

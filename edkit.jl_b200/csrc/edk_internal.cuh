@@ -178,6 +178,7 @@ struct edk_basis {
   std::vector<std::vector<int>> gen_perm;
   std::vector<std::vector<uint8_t>> gen_inv;
   bool phase_complex = false;
+  int device = 0;  // CUDA device the tables live on
   cudaStream_t stream = nullptr;
   std::mutex mu;
   ~edk_basis();
@@ -206,6 +207,8 @@ struct edk_operator {
 namespace edk {
 // implemented in edk_basis.cu
 edk_status check_basis_dev(const BasisDev& b);
+edk_status index_device(const BasisDev& dv, int64_t n, const uint64_t* s_d, int64_t* p_d,
+                        double2* c_d, cudaStream_t st);
 // implemented in edk_apply.cu
 edk_status apply_device(edk_operator* op, int dtype, const void* x, void* y, int64_t nvec,
                         int64_t ldx, int64_t ldy, int accumulate, cudaStream_t st);

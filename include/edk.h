@@ -110,6 +110,18 @@ edk_status edk_basis_export(const edk_basis* b, int64_t* I, double* R);
 edk_status edk_basis_index(const edk_basis* b, int64_t n, const uint64_t* states,
                            int64_t* pos, double* coeff, int32_t ptr_kind);
 
+/* index() for host-resident states without any device allocation: the same
+ * results as edk_basis_index(..., EDK_HOST), staged through a fixed 2 MiB
+ * scratch area inside the library (at most 65536 states per call; larger n is
+ * rejected with EDK_INVALID_ARG).  For callers that cannot allocate device
+ * memory where they need a lookup, such as code running during CUDA-graph
+ * capture or host callbacks that forbid allocation.  The scratch address is
+ * resolved on the first call for each device, so make that first call before
+ * any stream capture; calls are serialised and synchronous.  This entry point
+ * has no counterpart in the reference. */
+edk_status edk_basis_index_noalloc(const edk_basis* b, int64_t n, const uint64_t* states,
+                                   int64_t* pos, double* coeff);
+
 /* Build an operator from merged local terms — operator() Operator.jl:56-78
  * after its site-list merge, trans_inv_operator() Operator.jl:102-108.
  * Term t acts on nsites[t] sites (1-based, concatenated in `sites`) with a
