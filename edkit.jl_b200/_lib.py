@@ -58,6 +58,8 @@ class LanczosDiag(C.Structure):
         ("steps", C.c_int32), ("steps_low", C.c_int32), ("matvecs", C.c_int32),
         ("breakdown", C.c_int32), ("seconds", C.c_double), ("seconds_matvec", C.c_double),
         ("seconds_reorth", C.c_double), ("residual", C.c_double),
+        ("seconds_setup", C.c_double), ("seconds_stage1", C.c_double),
+        ("seconds_refine", C.c_double), ("refine_rounds", C.c_int32), ("checks", C.c_int32),
     ]
 
 

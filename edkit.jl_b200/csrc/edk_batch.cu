@@ -1,8 +1,845 @@
-// edk_batch.cu — Lanczos over many independent operators (momentum sectors
-// of one chain, disorder instances).
+// edk_batch.cu — Lanczos over many independent operators in lockstep
+// (momentum sectors of one chain, disorder instances), and the single-operator
+// ground state as a batch of one.
+//
+// Every kernel of a step covers all operators of the batch in one launch: a
+// block owns a tile of one operator's rows (tile2op / chunk2op maps), reads
+// that operator's basis/term descriptors from a device array, and works on
+// its slice of the concatenated buffers.  The step index j, the recurrence
+// coefficients alpha/beta, 1/beta and the per-operator stop flags live on the
+// device, so a step has no host round trip: it is captured once into a CUDA
+// graph and replayed.  The host looks at alpha/beta only every check_every
+// steps (tridiagonal eigenvalues, convergence).  One step per operator q:
+//   wt_q = H_q v_j                       (row-gather matvec)
+//   s = V_q^H wt_q ; alpha_j = Re s_j     (CGS sweep 1, FP64 block partials)
+//   w_q = wt_q - V_q s
+//   u = V_q^H w_q ; w_q -= V_q u ; beta_j = ||w_q||   (sweep 2 + norm)
+//   lucky breakdown beta <= sqrt(eps) max(1, |alpha|) stops operator q
+//   v_{j+1} = w_q / beta_j
+// (classical Gram-Schmidt twice, as _lanczos_build! in
+// src/algorithms/TimeEvolution.jl:250-306, with its three-term recurrence
+// folded into the first sweep).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <map>
+#include <memory>
 #include <vector>
 
-#include "edk_internal.cuh"
+#include "edk_rows.cuh"
+
+namespace edk {
+
+namespace {
+
+constexpr int kTile = 256;          // rows per matvec / update tile
+constexpr int kChunk = 1024;        // rows per dots chunk (4 per thread)
+
+template <class T> struct IsCx;
+template <> struct IsCx<double> { static constexpr bool v = false; };
+template <> struct IsCx<double2> { static constexpr bool v = true; };
+template <> struct IsCx<float> { static constexpr bool v = false; };
+template <> struct IsCx<float2> { static constexpr bool v = true; };
+
+__device__ __forceinline__ double2 l2(const double* p) { return make_double2(*p, 0.0); }
+__device__ __forceinline__ double2 l2(const double2* p) { return *p; }
+__device__ __forceinline__ double2 l2(const float* p) { return make_double2((double)*p, 0.0); }
+__device__ __forceinline__ double2 l2(const float2* p) {
+  float2 v = *p;
+  return make_double2((double)v.x, (double)v.y);
+}
+__device__ __forceinline__ void s2(double* p, double2 v) { *p = v.x; }
+__device__ __forceinline__ void s2(double2* p, double2 v) { *p = v; }
+__device__ __forceinline__ void s2(float* p, double2 v) { *p = (float)v.x; }
+__device__ __forceinline__ void s2(float2* p, double2 v) { *p = make_float2((float)v.x, (float)v.y); }
+
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace
+
+// One operator of a batch, as the kernels see it.
+struct BOp {
+  BasisDev b;
+  OpDev op;
+  FFParams ff;
+  int64_t D;
+  int64_t voff;   // element offset of V_q (D x ncap, column-major)
+  int64_t woff;   // element offset into w / wt
+  int64_t pofs;   // offset of the dots partials (ncap x nchunk)
+  int64_t tile0;  // first matvec/update tile
+  int64_t chunk0; // first dots chunk
+  int ntile, nchunk;
+};
+
+// ---------------------------------------------------------------------------
+// kernels (j = *step; operators with done[q] != 0 are skipped)
+// ---------------------------------------------------------------------------
+template <int BK, class VT>
+__global__ void __launch_bounds__(256) k_bapply_ff(const BOp* __restrict__ ops,
+                                                   const int* __restrict__ tile2op,
+                                                   const VT* __restrict__ V, VT* __restrict__ wt,
+                                                   const int* __restrict__ step,
+                                                   const int* __restrict__ done) {
+  const int q = tile2op[blockIdx.x];
+  if (done[q]) return;
+  const BOp& o = ops[q];
+  const int j = *step;
+  ff_tile<BK, VT>(o.b, o.op, o.ff, (blockIdx.x - o.tile0) * (int64_t)kTile,
+                  V + o.voff + (int64_t)j * o.D, wt + o.woff, 0);
+}
+
+template <int BK, class VT>
+__global__ void __launch_bounds__(256) k_bapply_gen(const BOp* __restrict__ ops,
+                                                    const int* __restrict__ tile2op,
+                                                    const VT* __restrict__ V,
+                                                    VT* __restrict__ wt,
+                                                    const int* __restrict__ step,
+                                                    const int* __restrict__ done) {
+  __shared__ uint32_t s_binom[32 * 33];
+  if constexpr (BK == BK_PROJ_RANK) {
+    fill_binom32(s_binom);
+    __syncthreads();
+  }
+  const int q = tile2op[blockIdx.x];
+  if (done[q]) return;
+  const BOp& o = ops[q];
+  const int64_t i = (blockIdx.x - o.tile0) * (int64_t)kTile + threadIdx.x;
+  if (i >= o.D) return;
+  const int j = *step;
+  gen_row<BK, uint32_t, VT, true>(o.b, o.op, i, V + o.voff + (int64_t)j * o.D, wt + o.woff, 0,
+                                  s_binom);
+}
+
+// part[pofs + c * nchunk + chunk] = sum_{rows of chunk} conj(V_q[r, c]) w_q[r],  c <= j
+template <class VV, class WV>
+__global__ void __launch_bounds__(256) k_bdots(const BOp* __restrict__ ops,
+                                               const int* __restrict__ chunk2op,
+                                               const VV* __restrict__ V,
+                                               const WV* __restrict__ w,
+                                               double2* __restrict__ part,
+                                               const int* __restrict__ step,
+                                               const int* __restrict__ done) {
+  extern __shared__ double2 s_part[];
+  constexpr bool CX = IsCx<VV>::v || IsCx<WV>::v;
+  const int q = chunk2op[blockIdx.x];
+  if (done[q]) return;
+  const BOp& o = ops[q];
+  const int ncols = *step + 1;
+  const int64_t chunk = blockIdx.x - o.chunk0;
+  const int64_t r0 = chunk * kChunk;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t D = o.D;
+  const VV* Vq = V + o.voff;
+  const WV* wq = w + o.woff;
+  double2 wv[4];
+  int64_t rows[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    rows[k] = r0 + threadIdx.x + (int64_t)k * 256;
+    wv[k] = rows[k] < D ? l2(wq + rows[k]) : make_double2(0.0, 0.0);
+  }
+  for (int c = 0; c < ncols; ++c) {
+    const VV* Vc = Vq + (int64_t)c * D;
+    double ar = 0.0, ai = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (rows[k] < D) {
+        const double2 v = l2(Vc + rows[k]);
+        ar += v.x * wv[k].x + v.y * wv[k].y;
+        if (CX) ai += v.x * wv[k].y - v.y * wv[k].x;
+      }
+    }
+    ar = wsum(ar);
+    if (CX) ai = wsum(ai);
+    if (lane == 0) s_part[warp * ncols + c] = make_double2(ar, ai);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+    double sr = 0.0, si = 0.0;
+#pragma unroll
+    for (int ww = 0; ww < 8; ++ww) {
+      sr += s_part[ww * ncols + c].x;
+      si += s_part[ww * ncols + c].y;
+    }
+    part[o.pofs + (int64_t)c * o.nchunk + chunk] = make_double2(sr, si);
+  }
+}
+
+// coef[q * ncap + c] = sum over the chunks of operator q (one block per operator)
+__global__ void __launch_bounds__(256) k_breduce(const BOp* __restrict__ ops, int ncap,
+                                                 const double2* __restrict__ part,
+                                                 double2* __restrict__ coef,
+                                                 const int* __restrict__ step,
+                                                 const int* __restrict__ done) {
+  const int q = blockIdx.x;
+  if (done[q]) return;
+  const BOp& o = ops[q];
+  const int ncols = *step + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int c = warp; c < ncols; c += 8) {
+    const double2* pc = part + o.pofs + (int64_t)c * o.nchunk;
+    double sr = 0.0, si = 0.0;
+    for (int k = lane; k < o.nchunk; k += 32) {
+      const double2 v = pc[k];
+      sr += v.x;
+      si += v.y;
+    }
+    sr = wsum(sr);
+    si = wsum(si);
+    if (lane == 0) coef[(int64_t)q * ncap + c] = make_double2(sr, si);
+  }
+}
+
+// wout_q = win_q - V_q[:, 0:ncols] coef_q ; normpart[tile] = sum |wout|^2
+// ncols = *step + 1 (or 0 with zero_cols)
+template <class VV, class WI, class WO>
+__global__ void __launch_bounds__(256) k_bupdate(const BOp* __restrict__ ops,
+                                                 const int* __restrict__ tile2op, int ncap,
+                                                 const VV* __restrict__ V,
+                                                 const double2* __restrict__ coef,
+                                                 const WI* __restrict__ win, WO* __restrict__ wout,
+                                                 double* __restrict__ normpart,
+                                                 const int* __restrict__ step,
+                                                 const int* __restrict__ done, int zero_cols) {
+  extern __shared__ double2 s_coef[];
+  constexpr bool CX = IsCx<VV>::v || IsCx<WI>::v;
+  const int q = tile2op[blockIdx.x];
+  if (done[q]) return;
+  const BOp& o = ops[q];
+  const int ncols = zero_cols ? 0 : *step + 1;
+  for (int c = threadIdx.x; c < ncols; c += blockDim.x) s_coef[c] = coef[(int64_t)q * ncap + c];
+  __syncthreads();
+  const int64_t r = (blockIdx.x - o.tile0) * (int64_t)kTile + threadIdx.x;
+  double nrm = 0.0;
+  if (r < o.D) {
+    const VV* Vq = V + o.voff + r;
+    double2 acc = l2(win + o.woff + r);
+    int c = 0;
+    for (; c + 4 <= ncols; c += 4) {
+      const double2 v0 = l2(Vq + (int64_t)(c + 0) * o.D), v1 = l2(Vq + (int64_t)(c + 1) * o.D);
+      const double2 v2 = l2(Vq + (int64_t)(c + 2) * o.D), v3 = l2(Vq + (int64_t)(c + 3) * o.D);
+      const double2 k0 = s_coef[c], k1 = s_coef[c + 1], k2 = s_coef[c + 2], k3 = s_coef[c + 3];
+      acc.x -= v0.x * k0.x + v1.x * k1.x + v2.x * k2.x + v3.x * k3.x;
+      if (CX) {
+        acc.x += v0.y * k0.y + v1.y * k1.y + v2.y * k2.y + v3.y * k3.y;
+        acc.y -= v0.x * k0.y + v0.y * k0.x + v1.x * k1.y + v1.y * k1.x + v2.x * k2.y +
+                 v2.y * k2.x + v3.x * k3.y + v3.y * k3.x;
+      }
+    }
+    for (; c < ncols; ++c) {
+      const double2 v = l2(Vq + (int64_t)c * o.D), k = s_coef[c];
+      acc.x -= v.x * k.x;
+      if (CX) {
+        acc.x += v.y * k.y;
+        acc.y -= v.x * k.y + v.y * k.x;
+      }
+    }
+    s2(wout + o.woff + r, acc);
+    nrm = acc.x * acc.x + (CX ? acc.y * acc.y : 0.0);
+  }
+  if (normpart) {
+    __shared__ double s_n[8];
+    nrm = wsum(nrm);
+    if ((threadIdx.x & 31) == 0) s_n[threadIdx.x >> 5] = nrm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < 8; ++k) t += s_n[k];
+      normpart[blockIdx.x] = t;
+    }
+  }
+}
+
+// per operator: alpha_j, beta_j, breakdown, 1/beta (one block per operator)
+__global__ void __launch_bounds__(256) k_bfinish(const BOp* __restrict__ ops, int ncap, int m,
+                                                 const double* __restrict__ normpart,
+                                                 const double2* __restrict__ coef1,
+                                                 double* __restrict__ alpha,
+                                                 double* __restrict__ beta,
+                                                 double* __restrict__ invb,
+                                                 int* __restrict__ nsteps,
+                                                 const int* __restrict__ step,
+                                                 int* __restrict__ done, int setup) {
+  const int q = blockIdx.x;
+  if (done[q]) return;
+  const BOp& o = ops[q];
+  double s = 0.0;
+  for (int k = threadIdx.x; k < o.ntile; k += blockDim.x) s += normpart[o.tile0 + k];
+  __shared__ double sh[8];
+  s = wsum(s);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double n2 = 0.0;
+  for (int k = 0; k < 8; ++k) n2 += sh[k];
+  const double nrm = sqrt(n2);
+  if (setup) {  // starting vector: zero norm is an error for this operator
+    if (!(nrm > 0.0)) { done[q] = 3; invb[q] = 0.0; }
+    else invb[q] = 1.0 / nrm;
+    return;
+  }
+  const int j = *step;
+  const double a = coef1[(int64_t)q * ncap + j].x;
+  alpha[(int64_t)q * m + j] = a;
+  beta[(int64_t)q * m + j] = nrm;
+  nsteps[q] = j + 1;
+  const double seps = 1.4901161193847656e-08;  // sqrt(eps(Float64))
+  if (nrm <= seps * fmax(1.0, fabs(a))) {
+    beta[(int64_t)q * m + j] = 0.0;
+    done[q] = 2;
+    invb[q] = 0.0;
+  } else {
+    invb[q] = 1.0 / nrm;
+  }
+}
+
+// V_q[:, j+1] = w_q / beta (skipped past the last column)
+template <class WV, class VV>
+__global__ void __launch_bounds__(256) k_bscale(const BOp* __restrict__ ops,
+                                                const int* __restrict__ tile2op, int ncap,
+                                                const WV* __restrict__ w, VV* __restrict__ V,
+                                                const double* __restrict__ invb,
+                                                const int* __restrict__ step,
+                                                const int* __restrict__ done) {
+  const int q = tile2op[blockIdx.x];
+  if (done[q]) return;
+  const BOp& o = ops[q];
+  const int col = *step + 1;
+  if (col >= ncap) return;
+  const int64_t r = (blockIdx.x - o.tile0) * (int64_t)kTile + threadIdx.x;
+  if (r >= o.D) return;
+  const double sc = invb[q];
+  const double2 v = l2(w + o.woff + r);
+  s2(V + o.voff + (int64_t)col * o.D + r, make_double2(v.x * sc, v.y * sc));
+}
+
+__global__ void k_bnext(int* step) { *step += 1; }
+
+// out_q = V_q[:, 0:nc_q] c_q (coefficients per operator, FP64 output)
+template <class VV, class OV>
+__global__ void __launch_bounds__(256) k_bcombine(const BOp* __restrict__ ops,
+                                                  const int* __restrict__ tile2op, int ncap,
+                                                  const VV* __restrict__ V,
+                                                  const double2* __restrict__ c,
+                                                  const int* __restrict__ ncols,
+                                                  OV* __restrict__ out) {
+  const int q = tile2op[blockIdx.x];
+  const BOp& o = ops[q];
+  const int64_t r = (blockIdx.x - o.tile0) * (int64_t)kTile + threadIdx.x;
+  if (r >= o.D) return;
+  const int nc = ncols[q];
+  double ar = 0.0, ai = 0.0;
+  for (int k = 0; k < nc; ++k) {
+    const double2 v = l2(V + o.voff + (int64_t)k * o.D + r);
+    const double2 ck = c[(int64_t)q * ncap + k];
+    ar += v.x * ck.x - v.y * ck.y;
+    ai += v.x * ck.y + v.y * ck.x;
+  }
+  s2(out + o.woff + r, make_double2(ar, ai));
+}
+
+namespace {
+
+size_t esz(int dt) { return (dt == EDK_F64 || dt == EDK_C64) ? 8 : (dt == EDK_C128 ? 16 : 4); }
+
+template <class F> edk_status with_vt(int dt, F&& f) {
+  switch (dt) {
+    case EDK_F64: return f((double*)nullptr);
+    case EDK_C128: return f((double2*)nullptr);
+    case EDK_F32: return f((float*)nullptr);
+    case EDK_C64: return f((float2*)nullptr);
+  }
+  set_error("batch: unknown dtype");
+  return EDK_INVALID_ARG;
+}
+
+double wall() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// A batch of operators sharing a lookup kind, kernel family and storage type.
+struct BatchEngine {
+  int nops = 0, vdt = EDK_F64, wdt = EDK_F64, ncap = 0, m = 0;
+  int bk = 0;
+  bool ff = false;
+  cudaStream_t st = nullptr;
+  std::vector<BOp> hops;
+  std::vector<int64_t> Ds;
+  int64_t ntiles = 0, nchunks = 0, totalD = 0;
+  DevBuf dops, tile2op, chunk2op, V, w, wt, part, coef1, coef2, normpart, alpha, beta, invb,
+      done, step, nsteps, cbuf, cnc;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  bool graph_ok = false;
+
+  ~BatchEngine() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+
+  edk_status init(const std::vector<edk_operator*>& ops, int vdtype, int m_, int lookup_kind,
+                  bool use_ff, cudaStream_t s) {
+    nops = (int)ops.size();
+    vdt = vdtype;
+    wdt = (vdt == EDK_C128 || vdt == EDK_C64) ? EDK_C128 : EDK_F64;
+    m = m_;
+    ncap = m + 1;
+    bk = lookup_kind;
+    ff = use_ff;
+    st = s;
+    std::vector<int> t2o, c2o;
+    int64_t voff = 0, woff = 0, pofs = 0;
+    for (int q = 0; q < nops; ++q) {
+      edk_operator* op = ops[q];
+      BOp o{};
+      o.b = op->b->dev;
+      o.b.bk = bk;
+      o.op = op->dev;
+      if (use_ff) std::memcpy(&o.ff, op->ff_params.data(), sizeof(FFParams));
+      o.D = op->b->D;
+      o.ntile = (int)((o.D + kTile - 1) / kTile);
+      o.nchunk = (int)((o.D + kChunk - 1) / kChunk);
+      o.voff = voff;
+      o.woff = woff;
+      o.pofs = pofs;
+      o.tile0 = ntiles;
+      o.chunk0 = nchunks;
+      for (int k = 0; k < o.ntile; ++k) t2o.push_back(q);
+      for (int k = 0; k < o.nchunk; ++k) c2o.push_back(q);
+      ntiles += o.ntile;
+      nchunks += o.nchunk;
+      voff += o.D * ncap;
+      woff += o.D;
+      pofs += (int64_t)o.nchunk * ncap;
+      hops.push_back(o);
+      Ds.push_back(o.D);
+    }
+    totalD = woff;
+    EDK_RETURN_IF(dops.alloc_async(hops.size() * sizeof(BOp), st));
+    EDK_TRY_CUDA(cudaMemcpyAsync(dops.p, hops.data(), hops.size() * sizeof(BOp),
+                                 cudaMemcpyHostToDevice, st));
+    EDK_RETURN_IF(tile2op.alloc_async(t2o.size() * 4, st));
+    EDK_TRY_CUDA(cudaMemcpyAsync(tile2op.p, t2o.data(), t2o.size() * 4, cudaMemcpyHostToDevice, st));
+    EDK_RETURN_IF(chunk2op.alloc_async(c2o.size() * 4, st));
+    EDK_TRY_CUDA(cudaMemcpyAsync(chunk2op.p, c2o.data(), c2o.size() * 4, cudaMemcpyHostToDevice, st));
+    EDK_RETURN_IF(V.alloc_async((size_t)voff * esz(vdt), st));
+    EDK_RETURN_IF(w.alloc_async((size_t)totalD * esz(wdt), st));
+    EDK_RETURN_IF(wt.alloc_async((size_t)totalD * esz(vdt), st));
+    EDK_RETURN_IF(part.alloc_async((size_t)std::max<int64_t>(pofs, 1) * sizeof(double2), st));
+    EDK_RETURN_IF(coef1.alloc_async((size_t)nops * ncap * sizeof(double2), st));
+    EDK_RETURN_IF(coef2.alloc_async((size_t)nops * ncap * sizeof(double2), st));
+    EDK_RETURN_IF(normpart.alloc_async((size_t)ntiles * sizeof(double), st));
+    EDK_RETURN_IF(alpha.alloc_async((size_t)nops * m * sizeof(double), st));
+    EDK_RETURN_IF(beta.alloc_async((size_t)nops * m * sizeof(double), st));
+    EDK_RETURN_IF(invb.alloc_async((size_t)nops * sizeof(double), st));
+    EDK_RETURN_IF(done.alloc_async((size_t)nops * sizeof(int), st));
+    EDK_RETURN_IF(nsteps.alloc_async((size_t)nops * sizeof(int), st));
+    EDK_RETURN_IF(step.alloc_async(sizeof(int), st));
+    EDK_RETURN_IF(cbuf.alloc_async((size_t)nops * ncap * sizeof(double2), st));
+    EDK_RETURN_IF(cnc.alloc_async((size_t)nops * sizeof(int), st));
+    EDK_TRY_CUDA(cudaMemsetAsync(done.p, 0, nops * sizeof(int), st));
+    EDK_TRY_CUDA(cudaMemsetAsync(nsteps.p, 0, nops * sizeof(int), st));
+    EDK_TRY_CUDA(cudaMemsetAsync(alpha.p, 0, (size_t)nops * m * sizeof(double), st));
+    EDK_TRY_CUDA(cudaMemsetAsync(beta.p, 0, (size_t)nops * m * sizeof(double), st));
+    size_t dsm = (size_t)8 * ncap * sizeof(double2);
+    if (dsm > 227 * 1024) {
+      set_error("batch Lanczos: too many steps for the shared-memory reduction (max 1800)");
+      return EDK_UNSUPPORTED;
+    }
+    // large dynamic shared memory is opted into here, outside any capture
+    return with_vt(vdt, [&](auto vp) -> edk_status {
+      using VV = std::remove_pointer_t<decltype(vp)>;
+      return with_vt(wdt, [&](auto wp) -> edk_status {
+        using WD = std::remove_pointer_t<decltype(wp)>;
+        const size_t us = (size_t)ncap * sizeof(double2);
+        const auto kd1 = k_bdots<VV, VV>;
+        const auto kd2 = k_bdots<VV, WD>;
+        const auto ku1 = k_bupdate<VV, VV, WD>;
+        const auto ku2 = k_bupdate<VV, WD, WD>;
+        const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+        if (dsm > 48 * 1024) {
+          EDK_TRY_CUDA(cudaFuncSetAttribute(kd1, attr, (int)dsm));
+          EDK_TRY_CUDA(cudaFuncSetAttribute(kd2, attr, (int)dsm));
+        }
+        if (us > 48 * 1024) {
+          EDK_TRY_CUDA(cudaFuncSetAttribute(ku1, attr, (int)us));
+          EDK_TRY_CUDA(cudaFuncSetAttribute(ku2, attr, (int)us));
+        }
+        return EDK_OK;
+      });
+    });
+  }
+
+  const BOp* d_ops() const { return dops.as<BOp>(); }
+
+  edk_status launch_apply() {
+    const int* t2o = tile2op.as<int>();
+    const int* stp = step.as<int>();
+    const int* dn = done.as<int>();
+    return with_vt(vdt, [&](auto vp) -> edk_status {
+      using VT = std::remove_pointer_t<decltype(vp)>;
+      const VT* Vv = V.as<VT>();
+      VT* wv = wt.as<VT>();
+#define EDK_BAPPLY(BK)                                                                       \
+  case BK:                                                                                   \
+    if (ff) k_bapply_ff<BK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn); \
+    else k_bapply_gen<BK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);  \
+    break;
+      switch (bk) {
+        EDK_BAPPLY(BK_TENSOR)
+        EDK_BAPPLY(BK_PROJ_RANK)
+        EDK_BAPPLY(BK_PROJ_HASH)
+        EDK_BAPPLY(BK_TRANS0)
+        EDK_BAPPLY(BK_TRANS)
+        EDK_BAPPLY(BK_TRANSPAR)
+        default:
+          set_error("batch Lanczos: lookup kind not supported in batches");
+          return EDK_UNSUPPORTED;
+      }
+#undef EDK_BAPPLY
+      return EDK_OK;
+    });
+  }
+
+  template <class XT>
+  edk_status launch_dots(const XT* x) {
+    size_t smem = (size_t)8 * ncap * sizeof(double2);
+    return with_vt(vdt, [&](auto vp) -> edk_status {
+      using VV = std::remove_pointer_t<decltype(vp)>;
+      auto kern = k_bdots<VV, XT>;
+      kern<<<(unsigned)nchunks, 256, smem, st>>>(d_ops(), chunk2op.as<int>(), V.as<VV>(), x,
+                                                 part.as<double2>(), step.as<int>(), done.as<int>());
+      return EDK_OK;
+    });
+  }
+
+  template <class WI, class WO>
+  edk_status launch_update(const double2* coef, const WI* win, WO* wout, bool norm, int zero) {
+    size_t smem = (size_t)ncap * sizeof(double2);
+    return with_vt(vdt, [&](auto vp) -> edk_status {
+      using VV = std::remove_pointer_t<decltype(vp)>;
+      auto kern = k_bupdate<VV, WI, WO>;
+      kern<<<(unsigned)ntiles, 256, smem, st>>>(d_ops(), tile2op.as<int>(), ncap, V.as<VV>(),
+                                                coef, win, wout,
+                                                norm ? normpart.as<double>() : nullptr,
+                                                step.as<int>(), done.as<int>(), zero);
+      return EDK_OK;
+    });
+  }
+
+  // one Lanczos step for every live operator (graph-capturable)
+  edk_status enqueue_step() {
+    EDK_RETURN_IF(launch_apply());
+    edk_status s = with_vt(vdt, [&](auto vp) -> edk_status {
+      using VV = std::remove_pointer_t<decltype(vp)>;
+      return with_vt(wdt, [&](auto wp) -> edk_status {
+        using WD = std::remove_pointer_t<decltype(wp)>;
+        EDK_RETURN_IF(launch_dots<VV>(wt.as<VV>()));
+        k_breduce<<<nops, 256, 0, st>>>(d_ops(), ncap, part.as<double2>(), coef1.as<double2>(),
+                                        step.as<int>(), done.as<int>());
+        EDK_RETURN_IF((launch_update<VV, WD>(coef1.as<double2>(), wt.as<VV>(), w.as<WD>(), false, 0)));
+        EDK_RETURN_IF(launch_dots<WD>(w.as<WD>()));
+        k_breduce<<<nops, 256, 0, st>>>(d_ops(), ncap, part.as<double2>(), coef2.as<double2>(),
+                                        step.as<int>(), done.as<int>());
+        EDK_RETURN_IF((launch_update<WD, WD>(coef2.as<double2>(), w.as<WD>(), w.as<WD>(), true, 0)));
+        k_bfinish<<<nops, 256, 0, st>>>(d_ops(), ncap, m, normpart.as<double>(),
+                                        coef1.as<double2>(), alpha.as<double>(), beta.as<double>(),
+                                        invb.as<double>(), nsteps.as<int>(), step.as<int>(),
+                                        done.as<int>(), 0);
+        k_bscale<WD, VV><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), tile2op.as<int>(), ncap,
+                                                           w.as<WD>(), V.as<VV>(),
+                                                           invb.as<double>(), step.as<int>(),
+                                                           done.as<int>());
+        k_bnext<<<1, 1, 0, st>>>(step.as<int>());
+        return EDK_OK;
+      });
+    });
+    EDK_RETURN_IF(s);
+    EDK_TRY_CUDA(cudaGetLastError());
+    return EDK_OK;
+  }
+
+  // V[:, 0] = start / ||start||; start is FP64 (wdt) concatenated on the device
+  edk_status setup(const void* start_dev) {
+    int minus1 = -1;
+    EDK_TRY_CUDA(cudaMemcpyAsync(step.p, &minus1, sizeof(int), cudaMemcpyHostToDevice, st));
+    edk_status s = with_vt(vdt, [&](auto vp) -> edk_status {
+      using VV = std::remove_pointer_t<decltype(vp)>;
+      return with_vt(wdt, [&](auto wp) -> edk_status {
+        using WD = std::remove_pointer_t<decltype(wp)>;
+        EDK_RETURN_IF((launch_update<WD, WD>(coef1.as<double2>(), (const WD*)start_dev,
+                                             w.as<WD>(), true, 1)));
+        k_bfinish<<<nops, 256, 0, st>>>(d_ops(), ncap, m, normpart.as<double>(),
+                                        coef1.as<double2>(), alpha.as<double>(), beta.as<double>(),
+                                        invb.as<double>(), nsteps.as<int>(), step.as<int>(),
+                                        done.as<int>(), 1);
+        k_bscale<WD, VV><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), tile2op.as<int>(), ncap,
+                                                           w.as<WD>(), V.as<VV>(),
+                                                           invb.as<double>(), step.as<int>(),
+                                                           done.as<int>());
+        k_bnext<<<1, 1, 0, st>>>(step.as<int>());
+        return EDK_OK;
+      });
+    });
+    EDK_RETURN_IF(s);
+    EDK_TRY_CUDA(cudaGetLastError());
+    return EDK_OK;
+  }
+
+  edk_status capture() {
+    if (graph_ok) return EDK_OK;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return EDK_OK;  // replay not available: launch directly
+    edk_status s = enqueue_step();
+    cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+    if (s != EDK_OK) return s;
+    if (e2 != cudaSuccess || !graph) { cudaGetLastError(); return EDK_OK; }
+    if (cudaGraphInstantiate(&gexec, graph, 0) != cudaSuccess) {
+      cudaGetLastError();
+      return EDK_OK;
+    }
+    graph_ok = true;
+    return EDK_OK;
+  }
+
+  edk_status run_step() {
+    if (graph_ok) {
+      EDK_TRY_CUDA(cudaGraphLaunch(gexec, st));
+      return EDK_OK;
+    }
+    return enqueue_step();
+  }
+};
+
+// Run the batch until every operator is done or max steps.
+edk_status run_batch(BatchEngine& E, int max_steps, int nev, double tol, int check_every,
+                     std::vector<OpResult>& res, int* nchecks = nullptr) {
+  const int nops = E.nops;
+  res.assign(nops, OpResult{});
+  std::vector<double> ha((size_t)nops * E.m), hb((size_t)nops * E.m);
+  std::vector<int> hdone(nops), hsteps(nops);
+  std::vector<std::vector<double>> prev(nops);
+  EDK_RETURN_IF(E.capture());
+  int every = check_every > 0 ? check_every : 10;
+  for (int j = 0; j < max_steps; ++j) {
+    EDK_RETURN_IF(E.run_step());
+    bool last = (j + 1 == max_steps);
+    if (!last && !((j + 1) % every == 0 && tol > 0)) continue;
+    if (nchecks) ++*nchecks;
+    EDK_TRY_CUDA(cudaMemcpyAsync(hdone.data(), E.done.p, nops * sizeof(int), cudaMemcpyDeviceToHost, E.st));
+    EDK_TRY_CUDA(cudaMemcpyAsync(hsteps.data(), E.nsteps.p, nops * sizeof(int), cudaMemcpyDeviceToHost, E.st));
+    EDK_TRY_CUDA(cudaMemcpyAsync(ha.data(), E.alpha.p, ha.size() * 8, cudaMemcpyDeviceToHost, E.st));
+    EDK_TRY_CUDA(cudaMemcpyAsync(hb.data(), E.beta.p, hb.size() * 8, cudaMemcpyDeviceToHost, E.st));
+    EDK_TRY_CUDA(cudaStreamSynchronize(E.st));
+    bool all_done = true;
+    bool changed = false;
+    for (int q = 0; q < nops; ++q) {
+      if (hdone[q]) continue;
+      int mq = hsteps[q];
+      if (tol > 0 && mq >= nev) {
+        std::vector<double> w(mq);
+        if (tridiag_eigvals(mq, ha.data() + (size_t)q * E.m, hb.data() + (size_t)q * E.m, w.data()) == 0) {
+          bool conv = !prev[q].empty();
+          for (int k = 0; k < nev && k < mq && conv; ++k)
+            conv = std::fabs(w[k] - prev[q][k]) <= tol * std::max(1.0, std::fabs(w[k]));
+          prev[q].assign(w.begin(), w.begin() + std::min(nev, mq));
+          if (conv) { hdone[q] = 1; changed = true; continue; }
+        }
+      }
+      all_done = false;
+    }
+    if (changed)
+      EDK_TRY_CUDA(cudaMemcpyAsync(E.done.p, hdone.data(), nops * sizeof(int), cudaMemcpyHostToDevice, E.st));
+    if (all_done) break;
+  }
+  EDK_TRY_CUDA(cudaMemcpyAsync(hdone.data(), E.done.p, nops * sizeof(int), cudaMemcpyDeviceToHost, E.st));
+  EDK_TRY_CUDA(cudaMemcpyAsync(hsteps.data(), E.nsteps.p, nops * sizeof(int), cudaMemcpyDeviceToHost, E.st));
+  EDK_TRY_CUDA(cudaMemcpyAsync(ha.data(), E.alpha.p, ha.size() * 8, cudaMemcpyDeviceToHost, E.st));
+  EDK_TRY_CUDA(cudaMemcpyAsync(hb.data(), E.beta.p, hb.size() * 8, cudaMemcpyDeviceToHost, E.st));
+  EDK_TRY_CUDA(cudaStreamSynchronize(E.st));
+  for (int q = 0; q < nops; ++q) {
+    OpResult& r = res[q];
+    r.status = hdone[q];
+    r.steps = hsteps[q];
+    r.a.assign(ha.begin() + (size_t)q * E.m, ha.begin() + (size_t)q * E.m + r.steps);
+    r.b.assign(hb.begin() + (size_t)q * E.m, hb.begin() + (size_t)q * E.m + r.steps);
+    if (r.steps > 0) {
+      std::vector<double> w(r.steps);
+      tridiag_eigvals(r.steps, r.a.data(), r.b.data(), w.data());
+      r.ev.assign(w.begin(), w.begin() + std::min(nev, r.steps));
+    }
+  }
+  return EDK_OK;
+}
+
+// FP64 Ritz vectors of the lowest Ritz value of each operator into out (wdt layout)
+edk_status ritz_vectors(BatchEngine& E, const std::vector<OpResult>& res, void* out) {
+  std::vector<double2> c((size_t)E.nops * E.ncap, make_double2(0.0, 0.0));
+  std::vector<int> nc(E.nops, 0);
+  for (int q = 0; q < E.nops; ++q) {
+    int mq = res[q].steps;
+    if (mq <= 0) continue;
+    std::vector<double> w(mq), Q((size_t)mq * mq);
+    if (tridiag_eigen(mq, res[q].a.data(), res[q].b.data(), w.data(), Q.data()) != 0) {
+      set_error("tridiagonal eigensolver did not converge");
+      return EDK_NOT_CONVERGED;
+    }
+    for (int k = 0; k < mq; ++k) c[(size_t)q * E.ncap + k] = make_double2(Q[k], 0.0);
+    nc[q] = mq;
+  }
+  const size_t cb = c.size() * sizeof(double2), nb = nc.size() * sizeof(int);
+  EDK_TRY_CUDA(cudaMemcpyAsync(E.cbuf.p, c.data(), cb, cudaMemcpyHostToDevice, E.st));
+  EDK_TRY_CUDA(cudaMemcpyAsync(E.cnc.p, nc.data(), nb, cudaMemcpyHostToDevice, E.st));
+  return with_vt(E.vdt, [&](auto vp) -> edk_status {
+    using VV = std::remove_pointer_t<decltype(vp)>;
+    return with_vt(E.wdt, [&](auto wp) -> edk_status {
+      using WD = std::remove_pointer_t<decltype(wp)>;
+      k_bcombine<VV, WD><<<(unsigned)E.ntiles, 256, 0, E.st>>>(
+          E.d_ops(), E.tile2op.as<int>(), E.ncap, E.V.as<VV>(), E.cbuf.as<double2>(),
+          E.cnc.as<int>(), (WD*)out);
+      EDK_TRY_CUDA(cudaGetLastError());
+      return EDK_OK;
+    });
+  });
+}
+
+// convert/copy concatenated start vectors into a device FP64 buffer of dtype wdt
+template <class S, class D>
+__global__ void k_cast(const S* __restrict__ src, int64_t n, D* __restrict__ dst) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    s2(dst + i, l2(src + i));
+}
+
+}  // namespace
+
+// Group-level driver: FP64 or mixed (FP32 Krylov vectors + FP64 refinement).
+edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczos_opts& o,
+                         const void* v0_dev, int v0_dt, cudaStream_t st,
+                         std::vector<OpResult>& res, edk_lanczos_diag* diag) {
+  double t0 = wall();
+  const int nops = (int)ops.size();
+  bool cx = o.complex_vectors != 0 || v0_dt == EDK_C128 || v0_dt == EDK_C64;
+  for (auto* op : ops) cx |= op->is_complex;
+  bool mixed = o.precision == EDK_PREC_MIXED;
+  int vdt = mixed ? (cx ? EDK_C64 : EDK_F32) : (cx ? EDK_C128 : EDK_F64);
+  int wdt = cx ? EDK_C128 : EDK_F64;
+  // common lookup kind: translation sectors with and without phases share BK_TRANS
+  int bk = ops[0]->b->dev.bk;
+  bool ff = true;
+  int64_t Dmin = INT64_MAX;
+  for (auto* op : ops) {
+    int k = op->b->dev.bk;
+    if (k != bk) {
+      if ((k == BK_TRANS0 || k == BK_TRANS) && (bk == BK_TRANS0 || bk == BK_TRANS)) bk = BK_TRANS;
+      else { set_error("batch Lanczos: operators of different basis kinds"); return EDK_UNSUPPORTED; }
+    }
+    ff = ff && op->ff_ok && op->use_ff;
+    if (!op->gather) {
+      set_error("batch Lanczos: an operator is not Hermitian in its basis");
+      return EDK_NOT_HERMITIAN;
+    }
+    if (op->b->L > 32) {
+      set_error("batch Lanczos: L > 32 is not supported");
+      return EDK_UNSUPPORTED;
+    }
+    Dmin = std::min<int64_t>(Dmin, op->b->D);
+  }
+  if (bk == BK_ABELIAN) { set_error("batch Lanczos: abelian bases run one at a time"); return EDK_UNSUPPORTED; }
+  (void)Dmin;  // operators smaller than max_steps stop by the breakdown rule
+  BatchEngine E;
+  double ts0 = wall();
+  int nchecks = 0;
+  EDK_RETURN_IF(E.init(ops, vdt, o.max_steps, bk, ff, st));
+  // start vectors in FP64 working dtype
+  DevBuf start;
+  EDK_RETURN_IF(start.alloc_async((size_t)E.totalD * esz(wdt), st));
+  edk_status s = with_vt(v0_dt, [&](auto sp) -> edk_status {
+    using SV = std::remove_pointer_t<decltype(sp)>;
+    return with_vt(wdt, [&](auto dp) -> edk_status {
+      using DV = std::remove_pointer_t<decltype(dp)>;
+      k_cast<SV, DV><<<1184, 256, 0, st>>>((const SV*)v0_dev, E.totalD, (DV*)start.p);
+      return EDK_OK;
+    });
+  });
+  EDK_RETURN_IF(s);
+  EDK_RETURN_IF(E.setup(start.p));
+  EDK_RETURN_IF(E.capture());
+  EDK_TRY_CUDA(cudaStreamSynchronize(st));
+  double ts1 = wall();
+  double tol1 = mixed ? std::max(o.tol, 1e-7) : o.tol;
+  EDK_RETURN_IF(run_batch(E, o.max_steps, o.nev, tol1, o.check_every, res, &nchecks));
+  double ts2 = wall();
+  int rounds = 0;
+  for (int q = 0; q < nops; ++q)
+    if (res[q].status == 3) {
+      set_error("Initial state has zero norm");
+      return EDK_ZERO_NORM;
+    }
+  int steps_low = 0, mvs = 0, bd = 0;
+  for (auto& r : res) { steps_low = std::max(steps_low, r.steps); mvs += r.steps; bd |= r.status == 2; }
+  if (mixed) {
+    // FP64 refinement rounds restarted from the Ritz vectors
+    int mr = o.refine_steps > 0 ? o.refine_steps : 20;
+    EDK_RETURN_IF(ritz_vectors(E, res, start.p));
+    for (int round = 0; round < 8; ++round) {
+      BatchEngine F;
+      EDK_RETURN_IF(F.init(ops, wdt, mr, bk, ff, st));
+      EDK_RETURN_IF(F.setup(start.p));
+      std::vector<OpResult> r2;
+      ++rounds;
+      EDK_RETURN_IF(run_batch(F, mr, o.nev, o.tol, std::min(5, mr), r2, &nchecks));
+      // a round is final when every operator converged (or broke down) inside
+      // it, or when it no longer moved the lowest Ritz value
+      bool done = true;
+      for (int q = 0; q < nops; ++q) {
+        double a = r2[q].ev.empty() ? 0.0 : r2[q].ev[0];
+        double b = res[q].ev.empty() ? 0.0 : res[q].ev[0];
+        bool inside = r2[q].status == 1 || r2[q].status == 2;
+        bool still = std::fabs(a - b) <= std::max(o.tol, 1e-14) * std::max(1.0, std::fabs(a));
+        if (!(inside || still)) done = false;
+        mvs += r2[q].steps;
+      }
+      res = r2;
+      if (done || o.nev > 1 || o.tol <= 0) break;
+      EDK_RETURN_IF(ritz_vectors(F, res, start.p));
+    }
+  }
+  EDK_TRY_CUDA(cudaStreamSynchronize(st));
+  if (diag) {
+    diag->steps = 0;
+    for (auto& r : res) diag->steps = std::max(diag->steps, r.steps);
+    diag->steps_low = mixed ? steps_low : diag->steps;
+    diag->matvecs = mvs;
+    diag->breakdown = bd;
+    diag->seconds = wall() - t0;
+    diag->seconds_matvec = NAN;
+    diag->seconds_reorth = NAN;
+    double resid = 0.0;
+    for (auto& r : res) {
+      int mm = r.steps;
+      if (mm <= 0) continue;
+      std::vector<double> w(mm), Q((size_t)mm * mm);
+      if (tridiag_eigen(mm, r.a.data(), r.b.data(), w.data(), Q.data()) == 0)
+        resid = std::max(resid, std::fabs(r.b[mm - 1] * Q[(size_t)mm - 1]));
+    }
+    diag->residual = resid;
+    diag->seconds_setup = ts1 - ts0;
+    diag->seconds_stage1 = ts2 - ts1;
+    diag->seconds_refine = mixed ? wall() - ts2 : 0.0;
+    diag->refine_rounds = rounds;
+    diag->checks = nchecks;
+  }
+  return EDK_OK;
+}
+
+}  // namespace edk
 
 using namespace edk;
 
@@ -10,28 +847,25 @@ extern "C" edk_status edk_batch_lanczos_e0(int32_t nops, edk_operator* const* op
                                            const edk_lanczos_opts* opts, const void* v0s,
                                            int32_t v0_dtype, double* evals,
                                            edk_lanczos_diag* diag) {
-  EDK_CHECK_ARG(nops >= 0 && ops && opts && v0s && evals, "edk_batch_lanczos_e0: NULL argument");
+  EDK_CHECK_ARG(nops >= 1 && ops && opts && v0s && evals, "edk_batch_lanczos_e0: NULL argument");
   EDK_CHECK_ARG(v0_dtype == EDK_F64 || v0_dtype == EDK_C128,
-                "edk_batch_lanczos_e0: v0s must be F64 or C128");
-  size_t es = v0_dtype == EDK_F64 ? 8 : 16;
-  size_t off = 0;
-  edk_lanczos_diag tot{};
-  for (int q = 0; q < nops; ++q) {
-    EDK_CHECK_ARG(ops[q] != nullptr, "edk_batch_lanczos_e0: NULL operator");
-    edk_lanczos_diag d{};
-    const char* v = static_cast<const char*>(v0s) + off;
-    EDK_RETURN_IF(edk_lanczos_e0(ops[q], opts, v, v0_dtype, EDK_HOST, evals + (size_t)q * opts->nev,
-                                 nullptr, nullptr, &d));
-    off += (size_t)ops[q]->b->D * es;
-    tot.steps = std::max(tot.steps, d.steps);
-    tot.steps_low = std::max(tot.steps_low, d.steps_low);
-    tot.matvecs += d.matvecs;
-    tot.breakdown |= d.breakdown;
-    tot.seconds += d.seconds;
-    tot.seconds_matvec += d.seconds_matvec;
-    tot.seconds_reorth += d.seconds_reorth;
-    tot.residual = std::max(tot.residual, d.residual);
+                "edk_batch_lanczos_e0: v0s must be F64 or C128 (host)");
+  EDK_CHECK_ARG(opts->max_steps >= 1 && opts->nev >= 1, "edk_batch_lanczos_e0: bad options");
+  std::vector<edk_operator*> v(ops, ops + nops);
+  int64_t tot = 0;
+  for (auto* op : v) {
+    EDK_CHECK_ARG(op != nullptr, "edk_batch_lanczos_e0: NULL operator");
+    tot += op->b->D;
   }
-  if (diag) *diag = tot;
+  cudaStream_t st = v[0]->stream;
+  size_t es = v0_dtype == EDK_F64 ? 8 : 16;
+  DevBuf v0d;
+  EDK_RETURN_IF(v0d.alloc((size_t)tot * es));
+  EDK_TRY_CUDA(cudaMemcpyAsync(v0d.p, v0s, (size_t)tot * es, cudaMemcpyHostToDevice, st));
+  std::vector<OpResult> res;
+  EDK_RETURN_IF(batch_lanczos(v, *opts, v0d.p, v0_dtype, st, res, diag));
+  for (int q = 0; q < nops; ++q)
+    for (int k = 0; k < opts->nev; ++k)
+      evals[(size_t)q * opts->nev + k] = k < (int)res[q].ev.size() ? res[q].ev[k] : NAN;
   return EDK_OK;
 }

@@ -46,19 +46,28 @@ const std::string& get_error();
     if (s_ != EDK_OK) return s_; \
   } while (0)
 
-// Owning device buffer.
+// Owning device buffer.  alloc() uses cudaMalloc; alloc_async() takes the
+// memory from the device's stream-ordered pool on stream `s` (workspace of the
+// Lanczos/Krylov drivers, reused across calls without new allocations).
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  cudaStream_t pool_stream = nullptr;
+  bool pooled = false;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (pooled) cudaFreeAsync(p, pool_stream);
+      else cudaFree(p);
+    }
     p = nullptr;
     bytes = 0;
+    pooled = false;
   }
+  edk_status alloc_async(size_t n, cudaStream_t s);
   edk_status alloc(size_t n) {
     release();
     if (n == 0) return EDK_OK;
@@ -74,6 +83,36 @@ struct DevBuf {
   }
   template <class T> T* as() const { return reinterpret_cast<T*>(p); }
 };
+
+// keep freed pool memory cached in the process (set once per device)
+inline void keep_pool_memory() {
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done[dev] = true;
+}
+
+inline edk_status DevBuf::alloc_async(size_t n, cudaStream_t s) {
+  release();
+  if (n == 0) return EDK_OK;
+  keep_pool_memory();
+  cudaError_t e = cudaMallocAsync(&p, n, s);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    set_error(std::string("cudaMallocAsync(") + std::to_string(n) + " bytes) failed: " +
+              cudaGetErrorString(e));
+    return EDK_OOM;
+  }
+  bytes = n;
+  pool_stream = s;
+  pooled = true;
+  return EDK_OK;
+}
 
 // ---------------------------------------------------------------------------
 // lookup / canonicalisation kinds (compile-time dispatch)
@@ -152,6 +191,18 @@ struct TermDev {
   int col_off;        // offset into colptr (2^nsites + 1 entries)
   int diag_off;       // offset into dval (2^nsites entries)
 };
+// Flip-flop bond families for the fast path (all 2-site off-diagonal terms
+// swap the two digits; every other term is diagonal).
+constexpr int kMaxFF = 4;
+struct FFParams {
+  int nfam;
+  int d[kMaxFF];
+  uint32_t valid[kMaxFF];
+  double2 dval[kMaxFF][4];
+  double2 v1[kMaxFF];  // M[2][1]: local column "01" -> row "10"
+  double2 v2[kMaxFF];  // M[1][2]: local column "10" -> row "01"
+};
+
 struct OpDev {
   int nfam;
   const FamDev* fam;
@@ -212,6 +263,15 @@ edk_status index_device(const BasisDev& dv, int64_t n, const uint64_t* s_d, int6
 // implemented in edk_apply.cu
 edk_status apply_device(edk_operator* op, int dtype, const void* x, void* y, int64_t nvec,
                         int64_t ldx, int64_t ldy, int accumulate, cudaStream_t st);
+// implemented in edk_batch.cu
+struct OpResult {
+  std::vector<double> a, b, ev;  // recurrence coefficients and lowest Ritz values
+  int steps = 0;
+  int status = 0;  // 0 ran to the step limit, 1 converged, 2 breakdown, 3 zero norm
+};
+edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczos_opts& o,
+                         const void* v0_dev, int v0_dt, cudaStream_t st,
+                         std::vector<OpResult>& res, edk_lanczos_diag* diag);
 // implemented in edk_util.cpp
 int tridiag_eigvals(int m, const double* a, const double* b, double* w);
 int tridiag_eigen(int m, const double* a, const double* b, double* w, double* Q);

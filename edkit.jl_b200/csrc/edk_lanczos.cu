@@ -537,6 +537,27 @@ extern "C" edk_status edk_lanczos_e0(edk_operator* op, const edk_lanczos_opts* o
   cudaStream_t st = op->stream;
   const int64_t D = op->b->D;
   EDK_CHECK_ARG(D >= 1, "edk_lanczos_e0: empty basis");
+  if (op->b->L <= 32 && op->b->dev.bk != BK_ABELIAN && opts->reorth) {
+    // batch of one: device-side recurrence, graph-replayed steps
+    DevBuf v0d;
+    size_t es = (v0_dtype == EDK_F64 || v0_dtype == EDK_C64) ? 8 : (v0_dtype == EDK_C128 ? 16 : 4);
+    const void* src = v0;
+    if (ptr_kind == EDK_HOST) {
+      EDK_RETURN_IF(v0d.alloc((size_t)D * es));
+      EDK_TRY_CUDA(cudaMemcpyAsync(v0d.p, v0, (size_t)D * es, cudaMemcpyHostToDevice, st));
+      src = v0d.p;
+    }
+    edk_lanczos_opts o = *opts;
+    o.max_steps = (int)std::min<int64_t>(o.max_steps, D);
+    std::vector<OpResult> res;
+    std::vector<edk_operator*> one(1, op);
+    EDK_RETURN_IF(batch_lanczos(one, o, src, v0_dtype, st, res, diag));
+    const OpResult& r = res[0];
+    for (int q = 0; q < opts->nev; ++q) evals[q] = q < (int)r.ev.size() ? r.ev[q] : NAN;
+    if (alpha) for (int q = 0; q < r.steps; ++q) alpha[q] = r.a[q];
+    if (beta) for (int q = 0; q < r.steps; ++q) beta[q] = r.b[q];
+    return EDK_OK;
+  }
   bool cx = op->is_complex || opts->complex_vectors || is_cx(v0_dtype);
   int m = std::min<int64_t>(opts->max_steps, D);
   bool mixed = opts->precision == EDK_PREC_MIXED;

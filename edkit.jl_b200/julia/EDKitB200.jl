@@ -40,7 +40,9 @@ end
 mutable struct LanczosDiag
     steps::Int32; steps_low::Int32; matvecs::Int32; breakdown::Int32
     seconds::Float64; seconds_matvec::Float64; seconds_reorth::Float64; residual::Float64
-    LanczosDiag() = new(0, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+    seconds_setup::Float64; seconds_stage1::Float64; seconds_refine::Float64
+    refine_rounds::Int32; checks::Int32
+    LanczosDiag() = new(0, 0, 0, 0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0, 0)
 end
 
 struct KrylovOpts

@@ -181,6 +181,11 @@ typedef struct {
   double seconds_matvec; /* time in matvec kernels (CUDA events) */
   double seconds_reorth; /* time in orthogonalisation kernels (CUDA events) */
   double residual;       /* |beta_m * y_m| of the lowest Ritz pair */
+  double seconds_setup;  /* workspace, start vector and step-graph set-up */
+  double seconds_stage1; /* first Lanczos stage (FP64, or FP32 storage when mixed) */
+  double seconds_refine; /* FP64 refinement stages (mixed precision) */
+  int32_t refine_rounds; /* FP64 refinement restarts taken */
+  int32_t checks;        /* host convergence checks */
 } edk_lanczos_diag;
 
 /* v0: starting vector (dtype v0_dtype, host or device); evals: nev values.
