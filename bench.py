@@ -195,6 +195,32 @@ def run_gpu(args):
     value = balg * world / (ms_step * 1e-3) / 1e9
     achieved = balg / (ms_mean * 1e-3) / 1e9
 
+    # the same product from the cached matrix (sparse!(opt) on the device)
+    mat = None
+    if not args.skip_materialized:
+        y_free = H * x.cpu().numpy()
+        entries = H.sparse_()
+        for _ in range(args.warmup):
+            flush.fill_(1.0)
+            matvec()
+        torch.cuda.synchronize()
+        evm = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            evm[i][0].record(stream)
+            matvec()
+            evm[i][1].record(stream)
+        torch.cuda.synchronize()
+        ms_m = float(np.mean([a.elapsed_time(c) for a, c in evm]))
+        ref_m = y_free
+        mat = {"ms_per_step": round(ms_m, 5), "GB_s_algorithmic": round(balg / ms_m / 1e6, 2),
+               "entries": entries, "stored_bytes": entries * 6 + D * 16,
+               "frac_of_measured_hbm": round(balg / ms_m / 1e6 / measured_peak()[0], 4),
+               "rel_diff_vs_matrix_free": float(
+                   np.linalg.norm(ref_m - y.cpu().numpy()) / np.linalg.norm(ref_m))}
+        H.clear_sparse_cache_()
+
     # end to end through the C ABI with pinned host buffers
     xh = torch.randn(D, dtype=torch.float64, generator=g).pin_memory()
     yh = torch.empty(D, dtype=torch.float64).pin_memory()
@@ -240,8 +266,14 @@ def run_gpu(args):
             "clocks": clk.summary(),
             "check_rel_err_vs_second_run": err,
         }
+        if mat is not None:
+            result["matvec_materialized"] = mat
         if not args.skip_e0:
             result["time_to_e0"] = time_to_e0(ek, H, D)
+        if args.extras:
+            result["config5_random_field_ensemble"] = config5_ensemble(ek)
+            result["config4_momentum_sectors"] = config4_sectors(ek)
+            result["config3_krylov_L32"] = config3_krylov(ek)
         if world == 1 and not args.skip_cpu:
             result["cpu_baseline"] = cpu_baseline(balg, D, budget_s=args.cpu_budget)
     if world > 1:
@@ -272,7 +304,106 @@ def time_to_e0(ek, H, D):
                     "refine_rounds": dmx["refine_rounds"], "checks": dmx["checks"], **phases(dmx)}
     out["dE0_rel_mixed_vs_fp64"] = abs(emx[0] - e64[0]) / abs(e64[0])
     out["speedup_mixed_vs_fp64"] = round(d64["seconds"] / dmx["seconds"], 3)
+    # same two runs on the cached matrix (sparse!(opt)); the build is timed too
+    t = time.perf_counter()
+    H.sparse_()
+    build = time.perf_counter() - t
+    for _ in range(2):
+        e64m, d64m = ek.lanczos_e0(H, v0, m=300, tol=1e-12, check_every=10)
+    for _ in range(2):
+        emxm, dmxm = ek.lanczos_e0(H, v0, m=300, tol=1e-12, check_every=10, precision="mixed",
+                                   refine_steps=20)
+    H.clear_sparse_cache_()
+    out["materialized"] = {
+        "build_seconds": round(build, 4),
+        "fp64_seconds": round(d64m["seconds"], 4), "mixed_seconds": round(dmxm["seconds"], 4),
+        "fp64_steps": d64m["steps"], "mixed_steps_fp32": dmxm["steps_low"],
+        "speedup_mixed_vs_fp64": round(d64m["seconds"] / dmxm["seconds"], 3),
+        "speedup_mixed_materialized_vs_fp64_matrix_free": round(d64["seconds"] / dmxm["seconds"], 3),
+        "dE0_rel_mixed_vs_fp64": abs(emxm[0] - e64[0]) / abs(e64[0])}
     return out
+
+
+def config5_ensemble(ek, n_inst=512, seed=2024, steps=200):
+    """512 random-field XXZ chains (open, Delta=1, h_i ~ U[-3,3] on spin-1/2 z),
+    L drawn from {12,14,16,18,20}, ProjectedBasis N=L/2: E0 and the gap ratio of
+    the four lowest Ritz values per instance, FP64 batched vs mixed batched, and
+    FP64 one instance at a time on a sample."""
+    rng = np.random.default_rng(seed)
+    bond = ek.spin((1.0, "xx"), (1.0, "yy"), (1.0, "zz"))
+    ops = []
+    for _ in range(n_inst):
+        Lq = int(rng.choice([12, 14, 16, 18, 20]))
+        h = rng.uniform(-3, 3, Lq)
+        mats = [bond] * (Lq - 1) + [hi * ek.spin("z") for hi in h]
+        inds = [[i, i + 1] for i in range(1, Lq)] + [[i] for i in range(1, Lq + 1)]
+        ops.append(ek.operator(mats, inds, ek.ProjectedBasis(L=Lq, N=Lq // 2)))
+    rows = sum(op.size(1) for op in ops)
+    v0s = [np.random.default_rng(q).standard_normal(op.size(1)) for q, op in enumerate(ops)]
+    res = {"instances": n_inst, "rows": rows}
+    for name, kw in (("fp64_batched", {}), ("mixed_batched", {"precision": "mixed"})):
+        for _ in range(2):
+            ev, d = ek.batch_lanczos_e0(ops, v0s, m=steps, nev=4, tol=1e-12, check_every=10, **kw)
+        res[name] = {"seconds": round(d["seconds"], 4), "max_steps": d["steps"],
+                     "matvecs": d["matvecs"]}
+        res[name + "_E0"] = ev[:, 0]
+    res["dE0_rel_max_mixed_vs_fp64"] = float(np.max(
+        np.abs(res["mixed_batched_E0"] - res["fp64_batched_E0"]) / np.abs(res["fp64_batched_E0"])))
+    res["mean_gap_ratio_low4"] = float(np.mean([np.mean(ek.gapratio(e)) for e in ev]))
+    ns = 32
+    t = time.perf_counter()
+    for q in range(ns):
+        ek.lanczos_e0(ops[q], v0s[q], m=steps, nev=4, tol=1e-12, check_every=10)
+    seq = (time.perf_counter() - t) * n_inst / ns
+    res["fp64_one_at_a_time_seconds_est"] = round(seq, 3)
+    res["speedup_mixed_batched_vs_fp64_one_at_a_time"] = round(seq / res["mixed_batched"]["seconds"], 2)
+    res["speedup_mixed_batched_vs_fp64_batched"] = round(
+        res["fp64_batched"]["seconds"] / res["mixed_batched"]["seconds"], 3)
+    del res["mixed_batched_E0"], res["fp64_batched_E0"]
+    return res
+
+
+def config4_sectors(ek, steps=100):
+    """Periodic XXZ L=26, Delta=1.5, N=13, all 26 momentum sectors in one batch:
+    the lowest 4 eigenvalues per sector (single-vector Lanczos per sector)."""
+    bond = ek.spin((1.0, "xx"), (1.0, "yy"), (1.5, "zz"))
+    ops = [ek.trans_inv_operator(bond, 2, ek.TranslationalBasis(L=26, N=13, k=k)) for k in range(26)]
+    res = {"sectors": 26, "dims": [op.size(1) for op in ops]}
+    for name, kw in (("fp64_batched", {}), ("mixed_batched", {"precision": "mixed"})):
+        for _ in range(2):
+            ev, d = ek.batch_lanczos_e0(ops, m=steps, nev=4, tol=1e-12, check_every=10, **kw)
+        res[name] = {"seconds": round(d["seconds"], 4), "max_steps": d["steps"]}
+        res[name + "_low4_k0"] = [float(v) for v in ev[0]]
+    res["E0_all_sectors"] = float(np.min(ev[:, 0]))
+    return res
+
+
+def config3_krylov(ek, ntimes=101):
+    """J1-J2 XXZ L=32 (J2=0.5), N=16, k=0 (D=18,784,170): Krylov exp(-iHt) psi0
+    from a seeded random product state, t = 0..10 step 0.1, m = 30; FP32 complex
+    Krylov vectors (mixed) vs FP64: fidelity and energy drift at the last time."""
+    b = ek.TranslationalBasis(L=32, N=16, k=0)
+    H = ek.trans_inv_operator(ek.spin((1.0, "xx"), (1.0, "yy"), (1.0, "zz")), 2, b) + \
+        ek.trans_inv_operator(ek.spin((0.5, "xx"), (0.5, "yy"), (0.5, "zz")), [1, 3], b)
+    rng = np.random.default_rng(99)
+    dg = np.zeros(32, dtype=np.int64)
+    dg[rng.choice(32, 16, replace=False)] = 1
+    psi0 = ek.productstate(dg, b).astype(np.complex128)
+    ts = np.round(np.arange(ntimes) * 0.1, 10)
+    res = {"D": b.size(1), "times": len(ts)}
+    out = {}
+    for name, prec in (("fp64", "fp64"), ("mixed", "mixed")):
+        psi, d = ek.timeevolve(H, psi0, ts[-1:], tol=1e-10, m_init=30, m_max=30,
+                               return_diagnostics=True, precision=prec)
+        res[name] = {"seconds": round(d.seconds, 3), "matvecs": d.matvecs,
+                     "restarts": d.restarts}
+        out[name] = psi[:, 0]
+    a, m = out["fp64"], out["mixed"]
+    res["fidelity_t10"] = float(abs(np.vdot(a, m)) ** 2 / (np.vdot(a, a).real * np.vdot(m, m).real))
+    e0 = float(np.vdot(psi0, H * psi0).real)
+    res["energy_drift_fp64"] = float(np.vdot(a, H * a).real / np.vdot(a, a).real - e0)
+    res["energy_drift_mixed"] = float(np.vdot(m, H * m).real / np.vdot(m, m).real - e0)
+    return res
 
 
 def cpu_sample(balg, D, budget_s, nthreads=0):
@@ -355,6 +486,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-e0", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-materialized", action="store_true")
+    ap.add_argument("--extras", action="store_true",
+                    help="also run the batched (configs 4, 5) and Krylov (config 3) workloads")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=120.0)
     args = ap.parse_args()

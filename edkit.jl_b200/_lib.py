@@ -23,6 +23,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 EXPORTS = [
     "edk_basis_create", "edk_basis_destroy", "edk_basis_dim", "edk_basis_export",
     "edk_basis_index", "edk_basis_index_noalloc", "edk_operator_create", "edk_operator_destroy", "edk_operator_info",
+    "edk_operator_materialize",
     "edk_apply", "edk_apply_async", "edk_lanczos_e0", "edk_krylov_default_opts",
     "edk_krylov_evolve", "edk_batch_lanczos_e0", "edk_tridiag_eigen", "edk_last_error",
     "edk_version",
@@ -103,6 +104,7 @@ def load():
         "edk_basis_index_noalloc": (st, [vp, i64, vp, vp, vp]),
         "edk_operator_create": (st, [vp, i32, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]),
         "edk_operator_destroy": (st, [vp]),
+        "edk_operator_materialize": (st, [vp, i32, C.POINTER(i64)]),
         "edk_operator_info": (st, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32),
                                    C.POINTER(i32)]),
         "edk_apply": (st, [vp, i32, vp, vp, i64, i64, i64, i32, i32]),

@@ -154,6 +154,7 @@ edk_status apply_device(edk_operator* op, int dtype, const void* x, void* y, int
     EDK_TRY_CUDA(cudaMemset2DAsync(y, ldy * es, 0, b.D * es, nvec, st));
   }
   bool sc = !op->gather;
+  if (op->sell_ok && !sc) return apply_sell(op, dtype, x, y, nvec, ldx, ldy, accumulate, st);
   if (op->ff_ok && !sc && op->use_ff) {
     const FFParams& ff = *reinterpret_cast<const FFParams*>(op->ff_params.data());
     switch (dtype) {

@@ -74,6 +74,7 @@ struct BOp {
   int64_t pofs;   // offset of the dots partials (ncap x nchunk)
   int64_t tile0;  // first matvec/update tile
   int64_t chunk0; // first dots chunk
+  int64_t sblk0;  // first block of the materialised-matrix product (8 slices each)
   int ntile, nchunk;
 };
 
@@ -92,6 +93,22 @@ __global__ void __launch_bounds__(256) k_bapply_ff(const BOp* __restrict__ ops,
   const int j = *step;
   ff_tile<BK, VT>(o.b, o.op, o.ff, (blockIdx.x - o.tile0) * (int64_t)kTile,
                   V + o.voff + (int64_t)j * o.D, wt + o.woff, 0);
+}
+
+template <class VT>
+__global__ void __launch_bounds__(256) k_bapply_sell(const BOp* __restrict__ ops,
+                                                     const int* __restrict__ sblk2op,
+                                                     const VT* __restrict__ V, VT* __restrict__ wt,
+                                                     const int* __restrict__ step,
+                                                     const int* __restrict__ done) {
+  const int q = sblk2op[blockIdx.x];
+  if (done[q]) return;
+  const BOp& o = ops[q];
+  const int64_t slice = (blockIdx.x - o.sblk0) * 8 + (threadIdx.x >> 5);
+  if (slice >= o.op.sell.nslices) return;
+  const int j = *step;
+  sell_slice<VT>(o.b, o.op.sell, slice, threadIdx.x & 31, V + o.voff + (int64_t)j * o.D,
+                 wt + o.woff, 0);
 }
 
 template <int BK, class VT>
@@ -368,11 +385,13 @@ struct BatchEngine {
   int nops = 0, vdt = EDK_F64, wdt = EDK_F64, ncap = 0, m = 0;
   int bk = 0;
   bool ff = false;
+  bool sell = false;
+  int64_t nsblk = 0;
   cudaStream_t st = nullptr;
   std::vector<BOp> hops;
   std::vector<int64_t> Ds;
   int64_t ntiles = 0, nchunks = 0, totalD = 0;
-  DevBuf dops, tile2op, chunk2op, V, w, wt, part, coef1, coef2, normpart, alpha, beta, invb,
+  DevBuf dops, tile2op, chunk2op, sblk2op, V, w, wt, part, coef1, coef2, normpart, alpha, beta, invb,
       done, step, nsteps, cbuf, cnc;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -393,8 +412,10 @@ struct BatchEngine {
     bk = lookup_kind;
     ff = use_ff;
     st = s;
-    std::vector<int> t2o, c2o;
+    std::vector<int> t2o, c2o, s2o;
     int64_t voff = 0, woff = 0, pofs = 0;
+    sell = true;
+    for (auto* op : ops) sell = sell && op->sell_ok;
     for (int q = 0; q < nops; ++q) {
       edk_operator* op = ops[q];
       BOp o{};
@@ -410,6 +431,12 @@ struct BatchEngine {
       o.pofs = pofs;
       o.tile0 = ntiles;
       o.chunk0 = nchunks;
+      o.sblk0 = nsblk;
+      if (sell) {
+        const int64_t nb = (op->dev.sell.nslices + 7) / 8;
+        for (int64_t k = 0; k < nb; ++k) s2o.push_back(q);
+        nsblk += nb;
+      }
       for (int k = 0; k < o.ntile; ++k) t2o.push_back(q);
       for (int k = 0; k < o.nchunk; ++k) c2o.push_back(q);
       ntiles += o.ntile;
@@ -427,6 +454,12 @@ struct BatchEngine {
     EDK_RETURN_IF(tile2op.alloc_async(t2o.size() * 4, st));
     EDK_TRY_CUDA(cudaMemcpyAsync(tile2op.p, t2o.data(), t2o.size() * 4, cudaMemcpyHostToDevice, st));
     EDK_RETURN_IF(chunk2op.alloc_async(c2o.size() * 4, st));
+    if (sell) {
+      EDK_RETURN_IF(sblk2op.alloc_async(std::max<size_t>(s2o.size(), 1) * 4, st));
+      if (!s2o.empty())
+        EDK_TRY_CUDA(cudaMemcpyAsync(sblk2op.p, s2o.data(), s2o.size() * 4,
+                                     cudaMemcpyHostToDevice, st));
+    }
     EDK_TRY_CUDA(cudaMemcpyAsync(chunk2op.p, c2o.data(), c2o.size() * 4, cudaMemcpyHostToDevice, st));
     EDK_RETURN_IF(V.alloc_async((size_t)voff * esz(vdt), st));
     EDK_RETURN_IF(w.alloc_async((size_t)totalD * esz(wdt), st));
@@ -486,6 +519,12 @@ struct BatchEngine {
       using VT = std::remove_pointer_t<decltype(vp)>;
       const VT* Vv = V.as<VT>();
       VT* wv = wt.as<VT>();
+      if (sell) {
+        if (nsblk > 0)
+          k_bapply_sell<VT><<<(unsigned)nsblk, 256, 0, st>>>(d_ops(), sblk2op.as<int>(), Vv, wv,
+                                                             stp, dn);
+        return EDK_OK;
+      }
 #define EDK_BAPPLY(BK)                                                                       \
   case BK:                                                                                   \
     if (ff) k_bapply_ff<BK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn); \
@@ -678,8 +717,10 @@ edk_status run_batch(BatchEngine& E, int max_steps, int nev, double tol, int che
   return EDK_OK;
 }
 
-// FP64 Ritz vectors of the lowest Ritz value of each operator into out (wdt layout)
-edk_status ritz_vectors(BatchEngine& E, const std::vector<OpResult>& res, void* out) {
+// FP64 start vectors for the refinement of each operator into out (wdt
+// layout): the sum of its `nev` lowest Ritz vectors, so the refined Krylov
+// space holds every wanted eigenvector.
+edk_status ritz_vectors(BatchEngine& E, const std::vector<OpResult>& res, void* out, int nev) {
   std::vector<double2> c((size_t)E.nops * E.ncap, make_double2(0.0, 0.0));
   std::vector<int> nc(E.nops, 0);
   for (int q = 0; q < E.nops; ++q) {
@@ -690,7 +731,12 @@ edk_status ritz_vectors(BatchEngine& E, const std::vector<OpResult>& res, void* 
       set_error("tridiagonal eigensolver did not converge");
       return EDK_NOT_CONVERGED;
     }
-    for (int k = 0; k < mq; ++k) c[(size_t)q * E.ncap + k] = make_double2(Q[k], 0.0);
+    const int nk = std::min(nev, mq);
+    for (int k = 0; k < mq; ++k) {
+      double v = 0.0;
+      for (int e = 0; e < nk; ++e) v += Q[k + (size_t)e * mq];
+      c[(size_t)q * E.ncap + k] = make_double2(v, 0.0);
+    }
     nc[q] = mq;
   }
   const size_t cb = c.size() * sizeof(double2), nb = nc.size() * sizeof(int);
@@ -787,7 +833,8 @@ edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczo
   if (mixed) {
     // FP64 refinement rounds restarted from the Ritz vectors
     int mr = o.refine_steps > 0 ? o.refine_steps : 20;
-    EDK_RETURN_IF(ritz_vectors(E, res, start.p));
+    if (o.nev > 1) mr = std::max(mr, 15 * o.nev);
+    EDK_RETURN_IF(ritz_vectors(E, res, start.p, o.nev));
     for (int round = 0; round < 8; ++round) {
       BatchEngine F;
       EDK_RETURN_IF(F.init(ops, wdt, mr, bk, ff, st));
@@ -799,16 +846,18 @@ edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczo
       // it, or when it no longer moved the lowest Ritz value
       bool done = true;
       for (int q = 0; q < nops; ++q) {
-        double a = r2[q].ev.empty() ? 0.0 : r2[q].ev[0];
-        double b = res[q].ev.empty() ? 0.0 : res[q].ev[0];
         bool inside = r2[q].status == 1 || r2[q].status == 2;
-        bool still = std::fabs(a - b) <= std::max(o.tol, 1e-14) * std::max(1.0, std::fabs(a));
+        bool still = r2[q].ev.size() == res[q].ev.size();
+        for (size_t k = 0; k < r2[q].ev.size() && still; ++k) {
+          const double a = r2[q].ev[k], b = res[q].ev[k];
+          still = std::fabs(a - b) <= std::max(o.tol, 1e-14) * std::max(1.0, std::fabs(a));
+        }
         if (!(inside || still)) done = false;
         mvs += r2[q].steps;
       }
       res = r2;
-      if (done || o.nev > 1 || o.tol <= 0) break;
-      EDK_RETURN_IF(ritz_vectors(F, res, start.p));
+      if (done || o.tol <= 0) break;
+      EDK_RETURN_IF(ritz_vectors(F, res, start.p, o.nev));
     }
   }
   EDK_TRY_CUDA(cudaStreamSynchronize(st));

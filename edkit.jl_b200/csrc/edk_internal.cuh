@@ -203,7 +203,26 @@ struct FFParams {
   double2 v2[kMaxFF];  // M[1][2]: local column "10" -> row "01"
 };
 
+// Materialised operator (the device counterpart of sparse!(opt)): sliced
+// ELLPACK with 32-row slices.  Rows are sorted by their number of nonzeros
+// inside windows of 256 rows; slice s holds rows rowid[32 s .. 32 s + 31] and
+// its entries k = 0..w_s-1 at off_s + 32 k + lane (lane = row in the slice):
+// col = target row, code = index into vt (vt[0] = 0 pads short rows).
+// y[r] = (1/R_r) sum conj(vt[code]) x[col] + conj(diag[r]) x[r].
+struct SellDev {
+  int64_t nslices;
+  const int* rowid;        // 32 per slice, -1 past the last row
+  const int64_t* off;      // entry offset of each slice
+  const int* width;        // entries per lane of each slice
+  const int* col;          // target rows
+  const uint16_t* code;    // coefficient codes
+  const double2* diag;     // diagonal per row
+  const double2* vt64;     // coefficient table, FP64
+  const float2* vt32;      // the same table rounded to FP32
+};
+
 struct OpDev {
+  SellDev sell;
   int nfam;
   const FamDev* fam;
   int nterm;
@@ -239,6 +258,10 @@ struct edk_operator {
   edk_basis* b = nullptr;
   edk::DevBuf fam, term, colptr, xmask, val, dval;
   edk::DevBuf hx, hy;  // staging buffers of edk_apply's host-pointer path (grow only)
+  // materialised matrix (edk_operator_materialize)
+  edk::DevBuf s_rowid, s_off, s_width, s_col, s_code, s_diag, s_vt64, s_vt32;
+  bool sell_ok = false;
+  int64_t sell_entries = 0;
   edk::OpDev dev{};
   bool gather = true;
   bool is_complex = false;
@@ -260,6 +283,9 @@ namespace edk {
 edk_status check_basis_dev(const BasisDev& b);
 edk_status index_device(const BasisDev& dv, int64_t n, const uint64_t* s_d, int64_t* p_d,
                         double2* c_d, cudaStream_t st);
+// implemented in edk_sell.cu
+edk_status apply_sell(edk_operator* op, int dtype, const void* x, void* y, int64_t nvec,
+                      int64_t ldx, int64_t ldy, int accumulate, cudaStream_t st);
 // implemented in edk_apply.cu
 edk_status apply_device(edk_operator* op, int dtype, const void* x, void* y, int64_t nvec,
                         int64_t ldx, int64_t ldy, int accumulate, cudaStream_t st);

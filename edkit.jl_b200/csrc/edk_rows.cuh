@@ -359,4 +359,48 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
 }
 
 
+// One 32-row slice of the materialised matrix (one warp).
+template <class VT>
+__device__ __forceinline__ void sell_slice(const BasisDev& b, const SellDev& sd, int64_t slice,
+                                           int lane, const VT* __restrict__ xk,
+                                           VT* __restrict__ yk, int accumulate) {
+  using A = typename VTraits<VT>::A;
+  constexpr bool CX = VTraits<VT>::cx;
+  const int row = __ldg(sd.rowid + slice * 32 + lane);
+  const int w = __ldg(sd.width + slice);
+  const int64_t base = __ldg(sd.off + slice) + lane;
+  A ar = 0, ai = 0;
+  for (int k = 0; k < w; ++k) {
+    const int c = __ldg(sd.col + base + (int64_t)k * 32);
+    const int code = __ldg(sd.code + base + (int64_t)k * 32);
+    A vr, vi;
+    if constexpr (sizeof(A) == 8) {
+      const double2 v = __ldg(sd.vt64 + code);
+      vr = v.x; vi = v.y;
+    } else {
+      const float2 v = __ldg(sd.vt32 + code);
+      vr = v.x; vi = v.y;
+    }
+    const Cx<A> xv = ldv(xk + c);
+    if constexpr (CX) {
+      ar += vr * xv.r + vi * xv.i;  // conj(v) * x
+      ai += vr * xv.i - vi * xv.r;
+    } else {
+      ar += vr * xv.r;
+    }
+  }
+  if (row < 0) return;
+  const A invR = b.R ? (A)(1.0 / __ldg(b.R + row)) : (A)1;
+  const double2 d = __ldg(sd.diag + row);
+  const Cx<A> xi = ldv(xk + row);
+  Cx<A> out{ar * invR + (A)d.x * xi.r + (A)d.y * xi.i, (A)0};
+  if constexpr (CX) out.i = ai * invR + (A)d.x * xi.i - (A)d.y * xi.r;
+  if (accumulate) {
+    const Cx<A> yo = ldout(yk + row);
+    out.r += yo.r;
+    out.i += yo.i;
+  }
+  stv(yk + row, out);
+}
+
 }  // namespace edk

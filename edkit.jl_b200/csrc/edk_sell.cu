@@ -1,0 +1,359 @@
+// edk_sell.cu — materialised operator: the device counterpart of EDKit's
+// sparse!(opt) cache (src/Operator.jl:221-285).
+//
+// The matrix-free kernels recompute every nonzero (orbit canonicalisation and
+// table probe) on every application.  An iterative solver applies the same H
+// hundreds of times, so it pays to expand the rows once: two passes of the
+// expansion (count, then fill) write a sliced-ELLPACK matrix (32-row slices,
+// rows sorted by length inside 256-row windows) whose entries are a 4-byte
+// target row and a 2-byte coefficient code.  The code indexes a small table of
+// distinct values val * phase * R[target]; 1/R[row] is applied per row.  The
+// product is then a streaming read of 6 bytes per nonzero plus the psi gather.
+#include <algorithm>
+#include <vector>
+
+#include "edk_rows.cuh"
+
+namespace edk {
+
+namespace {
+
+// (row, norm class, phase index) of one off-diagonal target, or false where
+// index() returns (0, 1).  Same canonicalisation as the matvec kernels.
+template <int BK>
+__device__ __forceinline__ bool sell_target(const BasisDev& b, uint32_t s, const uint32_t* binom,
+                                            int64_t& pos, int& cls, int& ph) {
+  const uint32_t mask = (uint32_t)b.maskL;
+  cls = 0;
+  ph = 0;
+  uint32_t key = s;
+  if constexpr (BK == BK_TENSOR) {
+    pos = s;
+    return true;
+  } else if constexpr (BK == BK_PROJ_RANK) {
+    if (__popc(s) != b.K) return false;
+    pos = colex_rank(s, binom);
+    return true;
+  } else {
+    if constexpr (BK == BK_TRANS0) {
+      key = canon_min32(s, b.L, b.A, b.len, mask);
+    } else if constexpr (BK == BK_TRANS) {
+      int M;
+      key = canon_arg32(s, b.L, b.A, b.len, mask, M);
+      ph = M;
+    } else if constexpr (BK == BK_TRANSPAR) {
+      uint32_t Iam, Ibm;
+      int Rr, M;
+      canon_par32(s, b.L, b.A, b.len, mask, Iam, Rr, Ibm, M);
+      double n;
+      if (Ibm < Iam) { key = Ibm; n = (double)b.P * __ldg(b.phase + M).x; }
+      else { key = Iam; n = __ldg(b.phase + Rr).x; }
+      ph = n < 0 ? 1 : 0;
+    }
+    uint32_t v;
+    if (!hash_find(b, key, v)) return false;
+    if (b.packed) { pos = (int64_t)(v >> 5); cls = (int)(v & 31u); }
+    else { pos = (int64_t)v; cls = 0; }
+    return true;
+  }
+}
+
+template <int BK>
+__global__ void __launch_bounds__(256) k_sell_count(BasisDev b, OpDev op, FFParams ff,
+                                                    uint8_t* __restrict__ cnt,
+                                                    double2* __restrict__ diag) {
+  __shared__ uint32_t s_binom[32 * 33];
+  if constexpr (BK == BK_PROJ_RANK) {
+    fill_binom32(s_binom);
+    __syncthreads();
+  }
+  const uint32_t mask = (uint32_t)b.maskL;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < b.D;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t st = (BK == BK_TENSOR) ? (uint32_t)i : (uint32_t)__ldg(b.I + i);
+    double dr = 0.0, di = 0.0;
+    int n = 0;
+    for (int f = 0; f < ff.nfam; ++f) {
+      const uint32_t X = st, Y = rotl_L(st, ff.d[f], b.L, mask), V = ff.valid[f];
+      const uint32_t m1 = ~X & Y & V, m2 = X & ~Y & V;
+      const int c0 = __popc(~X & ~Y & V), c1 = __popc(m1), c2 = __popc(m2), c3 = __popc(X & Y & V);
+      dr += ff.dval[f][0].x * c0 + ff.dval[f][1].x * c1 + ff.dval[f][2].x * c2 + ff.dval[f][3].x * c3;
+      di += ff.dval[f][0].y * c0 + ff.dval[f][1].y * c1 + ff.dval[f][2].y * c2 + ff.dval[f][3].y * c3;
+      uint32_t bits = m1 | m2;
+      while (bits) {
+        const int p = __ffs(bits) - 1;
+        bits &= bits - 1;
+        const int q = p >= ff.d[f] ? p - ff.d[f] : p - ff.d[f] + b.L;
+        int64_t pos;
+        int cls, ph;
+        if (sell_target<BK>(b, st ^ (1u << p) ^ (1u << q), s_binom, pos, cls, ph)) ++n;
+      }
+    }
+    for (int t = 0; t < op.nterm; ++t) {
+      const TermDev* T = op.term + t;
+      int c = 0;
+      for (int k = 0; k < T->nsites; ++k) c = (c << 1) | (int)((st >> T->bitpos[k]) & 1u);
+      const double2 dv = __ldg(op.dval + T->diag_off + c);
+      dr += dv.x;
+      di += dv.y;
+    }
+    cnt[i] = (uint8_t)n;
+    diag[i] = make_double2(dr, di);
+  }
+}
+
+template <int BK>
+__global__ void __launch_bounds__(256) k_sell_fill(BasisDev b, FFParams ff, int64_t nslices,
+                                                   const int* __restrict__ rowid,
+                                                   const int64_t* __restrict__ off,
+                                                   const int* __restrict__ width,
+                                                   int* __restrict__ col,
+                                                   uint16_t* __restrict__ code, int nph,
+                                                   int ncls) {
+  __shared__ uint32_t s_binom[32 * 33];
+  if constexpr (BK == BK_PROJ_RANK) {
+    fill_binom32(s_binom);
+    __syncthreads();
+  }
+  const uint32_t mask = (uint32_t)b.maskL;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < nslices * 32;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t slice = g >> 5;
+    const int lane = (int)(g & 31);
+    const int row = rowid[g];
+    const int w = width[slice];
+    const int64_t base = off[slice] + lane;
+    int k = 0;
+    if (row >= 0) {
+      const uint32_t st = (BK == BK_TENSOR) ? (uint32_t)row : (uint32_t)__ldg(b.I + row);
+      for (int f = 0; f < ff.nfam; ++f) {
+        const uint32_t X = st, Y = rotl_L(st, ff.d[f], b.L, mask), V = ff.valid[f];
+        uint32_t bits = (~X & Y & V) | (X & ~Y & V);
+        while (bits) {
+          const int p = __ffs(bits) - 1;
+          bits &= bits - 1;
+          const int q = p >= ff.d[f] ? p - ff.d[f] : p - ff.d[f] + b.L;
+          int64_t pos;
+          int cls, ph;
+          if (sell_target<BK>(b, st ^ (1u << p) ^ (1u << q), s_binom, pos, cls, ph) && k < w) {
+            const int val_id = 2 * f + (int)((st >> p) & 1u);
+            col[base + (int64_t)k * 32] = (int)pos;
+            code[base + (int64_t)k * 32] = (uint16_t)(1 + (val_id * nph + ph) * ncls + cls);
+            ++k;
+          }
+        }
+      }
+    }
+    for (; k < w; ++k) {  // padding: coefficient 0 on a valid row
+      col[base + (int64_t)k * 32] = row >= 0 ? row : 0;
+      code[base + (int64_t)k * 32] = 0;
+    }
+  }
+}
+
+template <class VT>
+__global__ void __launch_bounds__(256) k_sell_apply(BasisDev b, SellDev sd,
+                                                    const VT* __restrict__ x, VT* __restrict__ y,
+                                                    int64_t ldx, int64_t ldy, int accumulate) {
+  const int64_t slice = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (slice >= sd.nslices) return;
+  sell_slice<VT>(b, sd, slice, threadIdx.x & 31, x + (int64_t)blockIdx.y * ldx,
+                 y + (int64_t)blockIdx.y * ldy, accumulate);
+}
+
+int gridn(int64_t n) {
+  int64_t g = (n + 255) / 256;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
+}
+
+}  // namespace
+
+template <class VT>
+static edk_status launch_sell(const BasisDev& b, const SellDev& sd, const void* x, void* y,
+                              int64_t nvec, int64_t ldx, int64_t ldy, int accumulate,
+                              cudaStream_t st) {
+  for (int64_t k0 = 0; k0 < nvec; k0 += 65535) {
+    int64_t nk = std::min<int64_t>(nvec - k0, 65535);
+    dim3 grid((unsigned)((sd.nslices + 7) / 8), (unsigned)nk);
+    k_sell_apply<VT><<<grid, 256, 0, st>>>(b, sd, static_cast<const VT*>(x) + k0 * ldx,
+                                           static_cast<VT*>(y) + k0 * ldy, ldx, ldy, accumulate);
+    EDK_TRY_CUDA(cudaGetLastError());
+  }
+  return EDK_OK;
+}
+
+edk_status apply_sell(edk_operator* op, int dtype, const void* x, void* y, int64_t nvec,
+                      int64_t ldx, int64_t ldy, int accumulate, cudaStream_t st) {
+  const BasisDev& b = op->b->dev;
+  const SellDev& sd = op->dev.sell;
+  switch (dtype) {
+    case EDK_F64: return launch_sell<double>(b, sd, x, y, nvec, ldx, ldy, accumulate, st);
+    case EDK_C128: return launch_sell<double2>(b, sd, x, y, nvec, ldx, ldy, accumulate, st);
+    case EDK_F32: return launch_sell<float>(b, sd, x, y, nvec, ldx, ldy, accumulate, st);
+    case EDK_C64: return launch_sell<float2>(b, sd, x, y, nvec, ldx, ldy, accumulate, st);
+  }
+  set_error("apply: unknown dtype");
+  return EDK_INVALID_ARG;
+}
+
+static edk_status materialize(edk_operator* op) {
+  edk_basis* bb = op->b;
+  const BasisDev& b = bb->dev;
+  const int bk = b.bk;
+  if (!(op->ff_ok && op->gather && bb->L <= 32 &&
+        (bk == BK_TENSOR || bk == BK_PROJ_RANK || bk == BK_PROJ_HASH || bk == BK_TRANS0 ||
+         bk == BK_TRANS || bk == BK_TRANSPAR))) {
+    set_error("edk_operator_materialize: only Hermitian operators of XXZ-type bond families "
+              "(plus diagonal terms) on spin-1/2 bases with L <= 32 are materialised");
+    return EDK_UNSUPPORTED;
+  }
+  const bool symm = bk == BK_TRANS0 || bk == BK_TRANS || bk == BK_TRANSPAR;
+  if (symm && !b.packed) {
+    set_error("edk_operator_materialize: too many distinct orbit norms for coefficient codes");
+    return EDK_UNSUPPORTED;
+  }
+  const FFParams& ff = *reinterpret_cast<const FFParams*>(op->ff_params.data());
+  const int nval = 2 * ff.nfam;
+  const int nph = (bk == BK_TRANS) ? b.len : (bk == BK_TRANSPAR ? 2 : 1);
+  const int ncls = symm ? std::max(1, b.nclass) : 1;
+  const int64_t ncode = 1 + (int64_t)nval * nph * ncls;
+  if (ncode > 65535) {
+    set_error("edk_operator_materialize: more than 65535 distinct coefficients");
+    return EDK_UNSUPPORTED;
+  }
+  cudaStream_t st = op->stream;
+  const int64_t D = b.D;
+  DevBuf cnt;
+  EDK_RETURN_IF(cnt.alloc(std::max<int64_t>(D, 1)));
+  EDK_RETURN_IF(op->s_diag.alloc(std::max<int64_t>(D, 1) * sizeof(double2)));
+#define EDK_CNT(BK)                                                                             \
+  case BK:                                                                                      \
+    k_sell_count<BK><<<gridn(D), 256, 0, st>>>(b, op->dev, ff, cnt.as<uint8_t>(),              \
+                                               op->s_diag.as<double2>());                      \
+    break;
+  switch (bk) {
+    EDK_CNT(BK_TENSOR)
+    EDK_CNT(BK_PROJ_RANK)
+    EDK_CNT(BK_PROJ_HASH)
+    EDK_CNT(BK_TRANS0)
+    EDK_CNT(BK_TRANS)
+    EDK_CNT(BK_TRANSPAR)
+  }
+#undef EDK_CNT
+  EDK_TRY_CUDA(cudaGetLastError());
+  std::vector<uint8_t> hc(D);
+  if (D > 0) EDK_TRY_CUDA(cudaMemcpyAsync(hc.data(), cnt.p, D, cudaMemcpyDeviceToHost, st));
+  EDK_TRY_CUDA(cudaStreamSynchronize(st));
+  // rows sorted by length (descending) inside windows of 256 rows
+  const int64_t nwin = (D + 255) / 256;
+  const int64_t nslices = nwin * 8;
+  std::vector<int> rowid((size_t)nslices * 32, -1), width(nslices, 0);
+  std::vector<int64_t> off(nslices, 0);
+  int64_t E = 0;
+  for (int64_t wdx = 0; wdx < nwin; ++wdx) {
+    const int64_t r0 = wdx * 256, r1 = std::min<int64_t>(D, r0 + 256);
+    int bins[257] = {0};
+    for (int64_t r = r0; r < r1; ++r) bins[256 - hc[r]]++;
+    int start[257];
+    int acc = 0;
+    for (int k = 0; k < 257; ++k) { start[k] = acc; acc += bins[k]; }
+    for (int64_t r = r0; r < r1; ++r) rowid[(size_t)wdx * 256 + start[256 - hc[r]]++] = (int)r;
+    for (int sl = 0; sl < 8; ++sl) {
+      const int64_t s = wdx * 8 + sl;
+      const int first = rowid[(size_t)s * 32];
+      width[s] = first >= 0 ? hc[first] : 0;
+      off[s] = E;
+      E += (int64_t)width[s] * 32;
+    }
+  }
+  EDK_RETURN_IF(op->s_rowid.alloc(rowid.size() * sizeof(int)));
+  EDK_RETURN_IF(op->s_width.alloc(width.size() * sizeof(int)));
+  EDK_RETURN_IF(op->s_off.alloc(off.size() * sizeof(int64_t)));
+  EDK_RETURN_IF(op->s_col.alloc(std::max<int64_t>(E, 1) * sizeof(int)));
+  EDK_RETURN_IF(op->s_code.alloc(std::max<int64_t>(E, 1) * sizeof(uint16_t)));
+  EDK_TRY_CUDA(cudaMemcpyAsync(op->s_rowid.p, rowid.data(), rowid.size() * sizeof(int),
+                               cudaMemcpyHostToDevice, st));
+  EDK_TRY_CUDA(cudaMemcpyAsync(op->s_width.p, width.data(), width.size() * sizeof(int),
+                               cudaMemcpyHostToDevice, st));
+  EDK_TRY_CUDA(cudaMemcpyAsync(op->s_off.p, off.data(), off.size() * sizeof(int64_t),
+                               cudaMemcpyHostToDevice, st));
+#define EDK_FILL(BK)                                                                            \
+  case BK:                                                                                      \
+    k_sell_fill<BK><<<gridn(nslices * 32), 256, 0, st>>>(                                       \
+        b, ff, nslices, op->s_rowid.as<int>(), op->s_off.as<int64_t>(), op->s_width.as<int>(), \
+        op->s_col.as<int>(), op->s_code.as<uint16_t>(), nph, ncls);                            \
+    break;
+  switch (bk) {
+    EDK_FILL(BK_TENSOR)
+    EDK_FILL(BK_PROJ_RANK)
+    EDK_FILL(BK_PROJ_HASH)
+    EDK_FILL(BK_TRANS0)
+    EDK_FILL(BK_TRANS)
+    EDK_FILL(BK_TRANSPAR)
+  }
+#undef EDK_FILL
+  EDK_TRY_CUDA(cudaGetLastError());
+  // coefficient table val * phase * R[target]
+  std::vector<double2> ph(nph, make_double2(1.0, 0.0));
+  if (bk == BK_TRANS && b.len > 0)
+    EDK_TRY_CUDA(cudaMemcpyAsync(ph.data(), b.phase, nph * sizeof(double2), cudaMemcpyDeviceToHost, st));
+  if (bk == BK_TRANSPAR) ph[1] = make_double2(-1.0, 0.0);
+  EDK_TRY_CUDA(cudaStreamSynchronize(st));
+  std::vector<double2> vt((size_t)ncode, make_double2(0.0, 0.0));
+  std::vector<float2> vt32((size_t)ncode, make_float2(0.f, 0.f));
+  for (int v = 0; v < nval; ++v) {
+    const int f = v / 2;
+    const double2 val = (v % 2 == 0) ? ff.v1[f] : ff.v2[f];
+    for (int p = 0; p < nph; ++p)
+      for (int c = 0; c < ncls; ++c) {
+        const double r = symm ? b.Rcls[c] : 1.0;
+        const double re = (val.x * ph[p].x - val.y * ph[p].y) * r;
+        const double im = (val.x * ph[p].y + val.y * ph[p].x) * r;
+        const size_t code = 1 + ((size_t)v * nph + p) * ncls + c;
+        vt[code] = make_double2(re, im);
+        vt32[code] = make_float2((float)re, (float)im);
+      }
+  }
+  EDK_RETURN_IF(op->s_vt64.alloc(vt.size() * sizeof(double2)));
+  EDK_RETURN_IF(op->s_vt32.alloc(vt32.size() * sizeof(float2)));
+  EDK_TRY_CUDA(cudaMemcpyAsync(op->s_vt64.p, vt.data(), vt.size() * sizeof(double2),
+                               cudaMemcpyHostToDevice, st));
+  EDK_TRY_CUDA(cudaMemcpyAsync(op->s_vt32.p, vt32.data(), vt32.size() * sizeof(float2),
+                               cudaMemcpyHostToDevice, st));
+  EDK_TRY_CUDA(cudaStreamSynchronize(st));
+  SellDev& sd = op->dev.sell;
+  sd.nslices = nslices;
+  sd.rowid = op->s_rowid.as<int>();
+  sd.off = op->s_off.as<int64_t>();
+  sd.width = op->s_width.as<int>();
+  sd.col = op->s_col.as<int>();
+  sd.code = op->s_code.as<uint16_t>();
+  sd.diag = op->s_diag.as<double2>();
+  sd.vt64 = op->s_vt64.as<double2>();
+  sd.vt32 = op->s_vt32.as<float2>();
+  op->sell_entries = E;
+  op->sell_ok = true;
+  return EDK_OK;
+}
+
+}  // namespace edk
+
+using namespace edk;
+
+extern "C" edk_status edk_operator_materialize(edk_operator* op, int32_t enable,
+                                               int64_t* entries) {
+  EDK_CHECK_ARG(op != nullptr, "edk_operator_materialize: NULL operator");
+  std::lock_guard<std::mutex> lk(op->mu);
+  if (!enable) {
+    op->sell_ok = false;
+    op->dev.sell = SellDev{};
+    op->s_rowid.release(); op->s_off.release(); op->s_width.release(); op->s_col.release();
+    op->s_code.release(); op->s_diag.release(); op->s_vt64.release(); op->s_vt32.release();
+    op->sell_entries = 0;
+    if (entries) *entries = 0;
+    return EDK_OK;
+  }
+  if (!op->sell_ok) EDK_RETURN_IF(materialize(op));
+  if (entries) *entries = op->sell_entries;
+  return EDK_OK;
+}

@@ -279,6 +279,20 @@ class Operator:
 
     __matmul__ = __mul__
 
+    def sparse_(self):
+        """sparse!(opt): cache the expanded matrix on the device (Operator.jl:269-273);
+        later products, Lanczos and Krylov runs on this operator use it.
+        Returns the number of stored entries."""
+        n = C.c_int64()
+        E.check(E.load().edk_operator_materialize(self._h, 1, C.byref(n)))
+        self.materialized = True
+        return int(n.value)
+
+    def clear_sparse_cache_(self):
+        """clear_sparse_cache!() for this operator (Operator.jl:283)."""
+        E.check(E.load().edk_operator_materialize(self._h, 0, None))
+        self.materialized = False
+
     def todense(self):
         """Array(opt) — Operator.jl:171-196 (H times the identity, small D only)."""
         D = self.B.size(1)

@@ -141,6 +141,15 @@ edk_status edk_operator_destroy(edk_operator* op);
 edk_status edk_operator_info(const edk_operator* op, int32_t* gather, int32_t* is_complex,
                              int32_t* n_families, int32_t* n_generic);
 
+/* sparse!(opt) / clear_sparse_cache! (Operator.jl:221-285) for the device:
+ * enable=1 expands every row once into a cached sliced-ELLPACK matrix (4-byte
+ * target row + 2-byte coefficient code per nonzero) that every later
+ * edk_apply / edk_lanczos_e0 / edk_krylov_evolve / batch call on this operator
+ * uses; enable=0 frees it.  *entries (may be NULL) receives the number of
+ * stored entries.  Available for Hermitian operators built from XXZ-type bond
+ * families plus diagonal terms on spin-1/2 bases with L <= 32. */
+edk_status edk_operator_materialize(edk_operator* op, int32_t enable, int64_t* entries);
+
 /* y (+)= H x for an nvec-column block — mul!(y, H, x) Operator.jl:309-328
  * (accumulate=1) and H * x Operator.jl:372-394 (accumulate=0).  Synchronous:
  * returns when y is written (host or device). */

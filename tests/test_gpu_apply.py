@@ -207,3 +207,54 @@ def test_fast_path_matches_generic_kernel(ek, O, monkeypatch):
         assert rel(y1, ref) < 1e-12 and rel(y2, ref) < 1e-12
         if not H1.is_complex:
             assert rel(H1 * x.real.astype(np.float32), ref.real) < 2e-6
+
+
+def test_materialized_matrix_matches_oracle(ek, O):
+    """sparse!(opt): the cached sliced-ELL matrix gives the oracle's product on
+    every lookup kind, in FP64 and FP32 storage; clearing it restores the
+    matrix-free kernels."""
+    rng = np.random.default_rng(9)
+    L = 12
+    cases = [
+        (ek.TensorBasis(L=L), O.tensor(L)),
+        (ek.ProjectedBasis(L=L, N=6), O.projected(L, N=6)),
+        (ek.ProjectedBasis(L=L, N=6, f=lambda d: d[0] == 0), O.projected(L, N=6, f=lambda d: d[0] == 0)),
+        (ek.TranslationalBasis(L=L, k=0, N=6), O.translational(L, k=0, N=6)),
+        (ek.TranslationalBasis(L=L, k=5, N=6), O.translational(L, k=5, N=6)),
+        (ek.TranslationalBasis(L=L, k=1, a=2), O.translational(L, k=1, a=2)),
+        (ek.TranslationParityBasis(L=L, k=6, p=-1, N=6), O.transparity(L, k=6, p=-1, N=6)),
+    ]
+    j2 = ek.spin((0.5, "xx"), (0.5, "yy"), (0.3, "zz"))
+    for b, o in cases:
+        H = ek.trans_inv_operator(ek.spin(*XXZ), 2, b) + ek.trans_inv_operator(j2, [1, 3], b)
+        Ho = O.trans_inv_operator(O.spin(*XXZ), 2, o)
+        Ho2 = O.trans_inv_operator(O.spin((0.5, "xx"), (0.5, "yy"), (0.3, "zz")), [1, 3], o)
+        x = rng.standard_normal(b.size(1)) + 1j * rng.standard_normal(b.size(1))
+        ref = Ho.mul(x) + Ho2.mul(x)
+        y_free = H * x
+        n = H.sparse_()
+        assert n > 0
+        assert rel(H * x, ref) < 1e-12
+        assert rel(H * x.astype(np.complex64), ref) < 2e-6
+        if not H.is_complex:
+            assert rel(H * x.real.copy(), ref.real) < 1e-12
+        H.clear_sparse_cache_()
+        assert np.array_equal(H * x, y_free)
+
+
+def test_materialized_open_chain_with_fields(ek, O):
+    L = 14
+    rng = np.random.default_rng(10)
+    h = rng.uniform(-3, 3, L)
+    b, o = ek.ProjectedBasis(L=L, N=7), O.projected(L, N=7)
+    mats = [ek.spin(*XXZ)] * (L - 1) + [hi * ek.spin("z") for hi in h]
+    omats = [O.spin(*XXZ)] * (L - 1) + [hi * O.spin("z") for hi in h]
+    inds = [[i, i + 1] for i in range(1, L)] + [[i] for i in range(1, L + 1)]
+    H, Ho = ek.operator(mats, inds, b), O.operator(omats, inds, o)
+    H.sparse_()
+    x = rng.standard_normal(b.size(1))
+    assert rel(H * x, Ho.mul(x).real) < 1e-12
+    y0 = rng.standard_normal(b.size(1))
+    y = y0.copy()
+    ek.mul_(y, H, x)
+    assert rel(y, y0 + Ho.mul(x).real) < 1e-12

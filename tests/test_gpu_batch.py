@@ -75,3 +75,46 @@ def test_single_operator_matches_batch(ek):
     e1, _ = ek.lanczos_e0(H, v0, m=60)
     e2, _ = ek.batch_lanczos_e0([H], [v0], m=60)
     assert abs(e1[0] - e2[0, 0]) < 1e-13 * abs(e1[0])
+
+
+def test_mixed_precision_nev4_matches_fp64(ek, O):
+    """The four lowest eigenvalues of each sector agree between the mixed
+    (FP32 Krylov vectors + FP64 refinement) and the FP64 batched paths and the
+    dense spectrum."""
+    L = 14
+    ops, dense = [], []
+    for k in (0, 1, 7):
+        b = ek.TranslationalBasis(L=L, N=7, k=k)
+        ops.append(ek.trans_inv_operator(xxz(ek.spin, 1.5), 2, b))
+        Ho = O.trans_inv_operator(xxz(O.spin, 1.5), 2, O.translational(L, k=k, N=7))
+        dense.append(np.linalg.eigvalsh(Ho.dense())[:4])
+    emx, _ = ek.batch_lanczos_e0(ops, m=150, nev=4, tol=1e-12, check_every=5, precision="mixed")
+    e64, _ = ek.batch_lanczos_e0(ops, m=150, nev=4, tol=1e-12, check_every=5)
+    for q in range(3):
+        assert np.allclose(e64[q], dense[q], rtol=0, atol=1e-9 * abs(dense[q][0])), q
+        assert np.allclose(emx[q], dense[q], rtol=0, atol=1e-9 * abs(dense[q][0])), q
+
+
+def test_materialized_batch_and_krylov(ek, O):
+    """Lanczos batches and Krylov evolution on materialised operators give the
+    matrix-free results."""
+    L = 12
+    ops, refs = [], []
+    for k in range(L):
+        b = ek.TranslationalBasis(L=L, N=6, k=k)
+        H = ek.trans_inv_operator(xxz(ek.spin, 1.5), 2, b)
+        H.sparse_()
+        ops.append(H)
+        Ho = O.trans_inv_operator(xxz(O.spin, 1.5), 2, O.translational(L, k=k, N=6))
+        refs.append(np.linalg.eigvalsh(Ho.dense())[:2])
+    ev, _ = ek.batch_lanczos_e0(ops, m=80, nev=2, tol=1e-13, check_every=5)
+    for k in range(L):
+        assert np.allclose(ev[k], refs[k], rtol=0, atol=1e-10 * abs(refs[k][0])), k
+    H = ops[3]
+    rng = np.random.default_rng(3)
+    psi0 = rng.standard_normal(H.size(1)) + 1j * rng.standard_normal(H.size(1))
+    psi0 /= np.linalg.norm(psi0)
+    a = ek.timeevolve(H, psi0, [0.5, 2.0], tol=1e-11)
+    H.clear_sparse_cache_()
+    b_ = ek.timeevolve(H, psi0, [0.5, 2.0], tol=1e-11)
+    assert np.linalg.norm(a - b_) < 1e-9
