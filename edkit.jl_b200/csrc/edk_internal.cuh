@@ -207,10 +207,12 @@ struct FFParams {
 // ELLPACK with 32-row slices.  Rows are sorted by their number of nonzeros
 // inside windows of 256 rows; slice s holds rows rowid[32 s .. 32 s + 31] and
 // its entries k = 0..w_s-1 at off_s + 32 k + lane (lane = row in the slice):
-// col = target row, code = index into vt (vt[0] = 0 pads short rows).
+// col = target row, code = index into vt (vt[0] = 0 pads short rows); when
+// the code's bits and the row's bits fit together, both share one 32-bit word.
 // y[r] = (1/R_r) sum conj(vt[code]) x[col] + conj(diag[r]) x[r].
 struct SellDev {
   int64_t nslices;
+  int packed;              // > 0: entry = row << packed | code, both in `col`
   const int* rowid;        // 32 per slice, -1 past the last row
   const int64_t* off;      // entry offset of each slice
   const int* width;        // entries per lane of each slice

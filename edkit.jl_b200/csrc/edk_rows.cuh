@@ -370,9 +370,7 @@ __device__ __forceinline__ void sell_slice(const BasisDev& b, const SellDev& sd,
   const int w = __ldg(sd.width + slice);
   const int64_t base = __ldg(sd.off + slice) + lane;
   A ar = 0, ai = 0;
-  for (int k = 0; k < w; ++k) {
-    const int c = __ldg(sd.col + base + (int64_t)k * 32);
-    const int code = __ldg(sd.code + base + (int64_t)k * 32);
+  auto term = [&](int c, int code) {
     A vr, vi;
     if constexpr (sizeof(A) == 8) {
       const double2 v = __ldg(sd.vt64 + code);
@@ -388,6 +386,38 @@ __device__ __forceinline__ void sell_slice(const BasisDev& b, const SellDev& sd,
     } else {
       ar += vr * xv.r;
     }
+  };
+  const int* cp = sd.col + base;
+  int k = 0;
+  if (sd.packed) {
+    const unsigned* ep = reinterpret_cast<const unsigned*>(cp);
+    const int sh = sd.packed;
+    const unsigned cm = (1u << sh) - 1u;
+    for (; k + 4 <= w; k += 4) {  // four independent entries in flight
+      const unsigned e0 = __ldg(ep + (k + 0) * 32), e1 = __ldg(ep + (k + 1) * 32);
+      const unsigned e2 = __ldg(ep + (k + 2) * 32), e3 = __ldg(ep + (k + 3) * 32);
+      term((int)(e0 >> sh), (int)(e0 & cm));
+      term((int)(e1 >> sh), (int)(e1 & cm));
+      term((int)(e2 >> sh), (int)(e2 & cm));
+      term((int)(e3 >> sh), (int)(e3 & cm));
+    }
+    for (; k < w; ++k) {
+      const unsigned e = __ldg(ep + k * 32);
+      term((int)(e >> sh), (int)(e & cm));
+    }
+  } else {
+    const uint16_t* kp = sd.code + base;
+    for (; k + 4 <= w; k += 4) {
+      const int c0 = __ldg(cp + (k + 0) * 32), c1 = __ldg(cp + (k + 1) * 32);
+      const int c2 = __ldg(cp + (k + 2) * 32), c3 = __ldg(cp + (k + 3) * 32);
+      const int k0 = __ldg(kp + (k + 0) * 32), k1 = __ldg(kp + (k + 1) * 32);
+      const int k2 = __ldg(kp + (k + 2) * 32), k3 = __ldg(kp + (k + 3) * 32);
+      term(c0, k0);
+      term(c1, k1);
+      term(c2, k2);
+      term(c3, k3);
+    }
+    for (; k < w; ++k) term(__ldg(cp + k * 32), __ldg(kp + k * 32));
   }
   if (row < 0) return;
   const A invR = b.R ? (A)(1.0 / __ldg(b.R + row)) : (A)1;

@@ -8,7 +8,8 @@
 // rows sorted by length inside 256-row windows) whose entries are a 4-byte
 // target row and a 2-byte coefficient code.  The code indexes a small table of
 // distinct values val * phase * R[target]; 1/R[row] is applied per row.  The
-// product is then a streaming read of 6 bytes per nonzero plus the psi gather.
+// product is then a streaming read of 6 bytes per nonzero (4 when the row and
+// the code share one word) plus the psi gather.
 #include <algorithm>
 #include <vector>
 
@@ -109,7 +110,7 @@ __global__ void __launch_bounds__(256) k_sell_fill(BasisDev b, FFParams ff, int6
                                                    const int* __restrict__ width,
                                                    int* __restrict__ col,
                                                    uint16_t* __restrict__ code, int nph,
-                                                   int ncls) {
+                                                   int ncls, int packed) {
   __shared__ uint32_t s_binom[32 * 33];
   if constexpr (BK == BK_PROJ_RANK) {
     fill_binom32(s_binom);
@@ -137,16 +138,26 @@ __global__ void __launch_bounds__(256) k_sell_fill(BasisDev b, FFParams ff, int6
           int cls, ph;
           if (sell_target<BK>(b, st ^ (1u << p) ^ (1u << q), s_binom, pos, cls, ph) && k < w) {
             const int val_id = 2 * f + (int)((st >> p) & 1u);
-            col[base + (int64_t)k * 32] = (int)pos;
-            code[base + (int64_t)k * 32] = (uint16_t)(1 + (val_id * nph + ph) * ncls + cls);
+            const int cd = 1 + (val_id * nph + ph) * ncls + cls;
+            if (packed) {
+              col[base + (int64_t)k * 32] = (int)(((unsigned)pos << packed) | (unsigned)cd);
+            } else {
+              col[base + (int64_t)k * 32] = (int)pos;
+              code[base + (int64_t)k * 32] = (uint16_t)cd;
+            }
             ++k;
           }
         }
       }
     }
     for (; k < w; ++k) {  // padding: coefficient 0 on a valid row
-      col[base + (int64_t)k * 32] = row >= 0 ? row : 0;
-      code[base + (int64_t)k * 32] = 0;
+      const int r = row >= 0 ? row : 0;
+      if (packed) {
+        col[base + (int64_t)k * 32] = (int)((unsigned)r << packed);
+      } else {
+        col[base + (int64_t)k * 32] = r;
+        code[base + (int64_t)k * 32] = 0;
+      }
     }
   }
 }
@@ -269,8 +280,13 @@ static edk_status materialize(edk_operator* op) {
   EDK_RETURN_IF(op->s_rowid.alloc(rowid.size() * sizeof(int)));
   EDK_RETURN_IF(op->s_width.alloc(width.size() * sizeof(int)));
   EDK_RETURN_IF(op->s_off.alloc(off.size() * sizeof(int64_t)));
+  // packed entries: code in the low `cbits` bits, target row above them
+  int cbits = 1;
+  while ((int64_t(1) << cbits) < ncode) ++cbits;
+  const int packed = (D <= (int64_t(1) << (32 - cbits))) ? cbits : 0;
   EDK_RETURN_IF(op->s_col.alloc(std::max<int64_t>(E, 1) * sizeof(int)));
-  EDK_RETURN_IF(op->s_code.alloc(std::max<int64_t>(E, 1) * sizeof(uint16_t)));
+  if (!packed) EDK_RETURN_IF(op->s_code.alloc(std::max<int64_t>(E, 1) * sizeof(uint16_t)));
+  else op->s_code.release();
   EDK_TRY_CUDA(cudaMemcpyAsync(op->s_rowid.p, rowid.data(), rowid.size() * sizeof(int),
                                cudaMemcpyHostToDevice, st));
   EDK_TRY_CUDA(cudaMemcpyAsync(op->s_width.p, width.data(), width.size() * sizeof(int),
@@ -281,7 +297,7 @@ static edk_status materialize(edk_operator* op) {
   case BK:                                                                                      \
     k_sell_fill<BK><<<gridn(nslices * 32), 256, 0, st>>>(                                       \
         b, ff, nslices, op->s_rowid.as<int>(), op->s_off.as<int64_t>(), op->s_width.as<int>(), \
-        op->s_col.as<int>(), op->s_code.as<uint16_t>(), nph, ncls);                            \
+        op->s_col.as<int>(), op->s_code.as<uint16_t>(), nph, ncls, packed);                    \
     break;
   switch (bk) {
     EDK_FILL(BK_TENSOR)
@@ -323,6 +339,7 @@ static edk_status materialize(edk_operator* op) {
   EDK_TRY_CUDA(cudaStreamSynchronize(st));
   SellDev& sd = op->dev.sell;
   sd.nslices = nslices;
+  sd.packed = packed;
   sd.rowid = op->s_rowid.as<int>();
   sd.off = op->s_off.as<int64_t>();
   sd.width = op->s_width.as<int>();
