@@ -213,12 +213,15 @@ struct FFParams {
 struct SellDev {
   int64_t nslices;
   int packed;              // > 0: entry = row << packed | code, both in `col`
-  const int* rowid;        // 32 per slice, -1 past the last row
+  int rbits;               // slot word = row | norm class << rbits; ~0u past the last row
+  const unsigned* rowid;   // 32 per slice, in slot order
   const int64_t* off;      // entry offset of each slice
   const int* width;        // entries per lane of each slice
   const int* col;          // target rows
   const uint16_t* code;    // coefficient codes
-  const double2* diag;     // diagonal per row
+  const double* diag;      // real diagonal per slot (Hermitian operators with real terms)
+  const double2* diagc;    // complex diagonal per slot, or null
+  const double* rinv;      // 1 / R of each norm class (1 for bases without norms)
   const double2* vt64;     // coefficient table, FP64
   const float2* vt32;      // the same table rounded to FP32
 };
@@ -261,7 +264,7 @@ struct edk_operator {
   edk::DevBuf fam, term, colptr, xmask, val, dval;
   edk::DevBuf hx, hy;  // staging buffers of edk_apply's host-pointer path (grow only)
   // materialised matrix (edk_operator_materialize)
-  edk::DevBuf s_rowid, s_off, s_width, s_col, s_code, s_diag, s_vt64, s_vt32;
+  edk::DevBuf s_rowid, s_off, s_width, s_col, s_code, s_diag, s_vt64, s_vt32, s_rinv;
   bool sell_ok = false;
   int64_t sell_entries = 0;
   edk::OpDev dev{};

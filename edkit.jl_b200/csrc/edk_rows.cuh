@@ -359,69 +359,79 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
 }
 
 
-// One 32-row slice of the materialised matrix (one warp).
-template <class VT>
+// One 32-row slice of the materialised matrix (one warp, one row per lane).
+// The entry stream is read once (evict-first: it is not reused within the
+// product, psi is), four entries ahead of their psi gathers.  PACKED selects
+// the entry format at compile time (1: row << packed | code in one word,
+// 0: separate row and code arrays, -1: read sd.packed).  The diagonal operands
+// are loaded after the loop: hoisting them costs registers and occupancy.
+template <class VT, int PACKED = -1>
 __device__ __forceinline__ void sell_slice(const BasisDev& b, const SellDev& sd, int64_t slice,
                                            int lane, const VT* __restrict__ xk,
                                            VT* __restrict__ yk, int accumulate) {
   using A = typename VTraits<VT>::A;
   constexpr bool CX = VTraits<VT>::cx;
-  const int row = __ldg(sd.rowid + slice * 32 + lane);
+  const int64_t slot = slice * 32 + lane;
+  const unsigned rc = __ldg(sd.rowid + slot);
   const int w = __ldg(sd.width + slice);
   const int64_t base = __ldg(sd.off + slice) + lane;
   A ar = 0, ai = 0;
   auto term = [&](int c, int code) {
-    A vr, vi;
-    if constexpr (sizeof(A) == 8) {
-      const double2 v = __ldg(sd.vt64 + code);
-      vr = v.x; vi = v.y;
-    } else {
-      const float2 v = __ldg(sd.vt32 + code);
-      vr = v.x; vi = v.y;
-    }
     const Cx<A> xv = ldv(xk + c);
     if constexpr (CX) {
+      A vr, vi;
+      if constexpr (sizeof(A) == 8) {
+        const double2 v = __ldg(sd.vt64 + code);
+        vr = v.x; vi = v.y;
+      } else {
+        const float2 v = __ldg(sd.vt32 + code);
+        vr = v.x; vi = v.y;
+      }
       ar += vr * xv.r + vi * xv.i;  // conj(v) * x
       ai += vr * xv.i - vi * xv.r;
     } else {
+      A vr;
+      if constexpr (sizeof(A) == 8) vr = __ldg(reinterpret_cast<const double*>(sd.vt64) + 2 * code);
+      else vr = __ldg(reinterpret_cast<const float*>(sd.vt32) + 2 * code);
       ar += vr * xv.r;
     }
   };
-  const int* cp = sd.col + base;
   int k = 0;
-  if (sd.packed) {
-    const unsigned* ep = reinterpret_cast<const unsigned*>(cp);
+  if (PACKED == 1 || (PACKED < 0 && sd.packed)) {
+    const unsigned* ep = reinterpret_cast<const unsigned*>(sd.col + base);
     const int sh = sd.packed;
     const unsigned cm = (1u << sh) - 1u;
     for (; k + 4 <= w; k += 4) {  // four independent entries in flight
-      const unsigned e0 = __ldg(ep + (k + 0) * 32), e1 = __ldg(ep + (k + 1) * 32);
-      const unsigned e2 = __ldg(ep + (k + 2) * 32), e3 = __ldg(ep + (k + 3) * 32);
+      const unsigned e0 = __ldcs(ep + (k + 0) * 32), e1 = __ldcs(ep + (k + 1) * 32);
+      const unsigned e2 = __ldcs(ep + (k + 2) * 32), e3 = __ldcs(ep + (k + 3) * 32);
       term((int)(e0 >> sh), (int)(e0 & cm));
       term((int)(e1 >> sh), (int)(e1 & cm));
       term((int)(e2 >> sh), (int)(e2 & cm));
       term((int)(e3 >> sh), (int)(e3 & cm));
     }
     for (; k < w; ++k) {
-      const unsigned e = __ldg(ep + k * 32);
+      const unsigned e = __ldcs(ep + k * 32);
       term((int)(e >> sh), (int)(e & cm));
     }
-  } else {
+  } else if (PACKED <= 0) {
+    const int* cp = sd.col + base;
     const uint16_t* kp = sd.code + base;
     for (; k + 4 <= w; k += 4) {
-      const int c0 = __ldg(cp + (k + 0) * 32), c1 = __ldg(cp + (k + 1) * 32);
-      const int c2 = __ldg(cp + (k + 2) * 32), c3 = __ldg(cp + (k + 3) * 32);
-      const int k0 = __ldg(kp + (k + 0) * 32), k1 = __ldg(kp + (k + 1) * 32);
-      const int k2 = __ldg(kp + (k + 2) * 32), k3 = __ldg(kp + (k + 3) * 32);
+      const int c0 = __ldcs(cp + (k + 0) * 32), c1 = __ldcs(cp + (k + 1) * 32);
+      const int c2 = __ldcs(cp + (k + 2) * 32), c3 = __ldcs(cp + (k + 3) * 32);
+      const int k0 = __ldcs(kp + (k + 0) * 32), k1 = __ldcs(kp + (k + 1) * 32);
+      const int k2 = __ldcs(kp + (k + 2) * 32), k3 = __ldcs(kp + (k + 3) * 32);
       term(c0, k0);
       term(c1, k1);
       term(c2, k2);
       term(c3, k3);
     }
-    for (; k < w; ++k) term(__ldg(cp + k * 32), __ldg(kp + k * 32));
+    for (; k < w; ++k) term(__ldcs(cp + k * 32), __ldcs(kp + k * 32));
   }
-  if (row < 0) return;
-  const A invR = b.R ? (A)(1.0 / __ldg(b.R + row)) : (A)1;
-  const double2 d = __ldg(sd.diag + row);
+  if (rc == ~0u) return;
+  const int64_t row = rc & ((1u << sd.rbits) - 1u);
+  const A invR = (A)__ldg(sd.rinv + (rc >> sd.rbits));
+  const double2 d = sd.diagc ? __ldg(sd.diagc + slot) : make_double2(__ldg(sd.diag + slot), 0.0);
   const Cx<A> xi = ldv(xk + row);
   Cx<A> out{ar * invR + (A)d.x * xi.r + (A)d.y * xi.i, (A)0};
   if constexpr (CX) out.i = ai * invR + (A)d.x * xi.i - (A)d.y * xi.r;

@@ -7,9 +7,10 @@
 // expansion (count, then fill) write a sliced-ELLPACK matrix (32-row slices,
 // rows sorted by length inside 256-row windows) whose entries are a 4-byte
 // target row and a 2-byte coefficient code.  The code indexes a small table of
-// distinct values val * phase * R[target]; 1/R[row] is applied per row.  The
-// product is then a streaming read of 6 bytes per nonzero (4 when the row and
-// the code share one word) plus the psi gather.
+// distinct values val * phase * R[target]; 1/R[row] is applied per row from a
+// table of the norm classes.  The product is then a streaming read of 6 bytes
+// per nonzero (4 when the row and the code share one word) and 12 per row
+// (slot word, real diagonal) plus the psi gather.
 #include <algorithm>
 #include <vector>
 
@@ -105,7 +106,10 @@ __global__ void __launch_bounds__(256) k_sell_count(BasisDev b, OpDev op, FFPara
 
 template <int BK>
 __global__ void __launch_bounds__(256) k_sell_fill(BasisDev b, FFParams ff, int64_t nslices,
-                                                   const int* __restrict__ rowid,
+                                                   int* __restrict__ rowid,
+                                                   const double2* __restrict__ diag_rows,
+                                                   double* __restrict__ diag,
+                                                   double2* __restrict__ diagc, int rbits,
                                                    const int64_t* __restrict__ off,
                                                    const int* __restrict__ width,
                                                    int* __restrict__ col,
@@ -127,6 +131,17 @@ __global__ void __launch_bounds__(256) k_sell_fill(BasisDev b, FFParams ff, int6
     int k = 0;
     if (row >= 0) {
       const uint32_t st = (BK == BK_TENSOR) ? (uint32_t)row : (uint32_t)__ldg(b.I + row);
+      // slot word: the row and its own norm class (the class that index() of
+      // the representative returns); the diagonal moves to slot order
+      int64_t own;
+      int cls = 0, ph;
+      if constexpr (BK == BK_TRANS0 || BK == BK_TRANS || BK == BK_TRANSPAR) {
+        sell_target<BK>(b, st, nullptr, own, cls, ph);
+      }
+      rowid[g] = (int)((unsigned)row | ((unsigned)cls << rbits));
+      const double2 dv = diag_rows[row];
+      if (diagc) diagc[g] = dv;
+      else diag[g] = dv.x;
       for (int f = 0; f < ff.nfam; ++f) {
         const uint32_t X = st, Y = rotl_L(st, ff.d[f], b.L, mask), V = ff.valid[f];
         uint32_t bits = (~X & Y & V) | (X & ~Y & V);
@@ -150,6 +165,10 @@ __global__ void __launch_bounds__(256) k_sell_fill(BasisDev b, FFParams ff, int6
         }
       }
     }
+    if (row < 0) {
+      if (diagc) diagc[g] = make_double2(0.0, 0.0);
+      else diag[g] = 0.0;
+    }
     for (; k < w; ++k) {  // padding: coefficient 0 on a valid row
       const int r = row >= 0 ? row : 0;
       if (packed) {
@@ -162,14 +181,14 @@ __global__ void __launch_bounds__(256) k_sell_fill(BasisDev b, FFParams ff, int6
   }
 }
 
-template <class VT>
+template <class VT, int PACKED>
 __global__ void __launch_bounds__(256) k_sell_apply(BasisDev b, SellDev sd,
                                                     const VT* __restrict__ x, VT* __restrict__ y,
                                                     int64_t ldx, int64_t ldy, int accumulate) {
   const int64_t slice = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
   if (slice >= sd.nslices) return;
-  sell_slice<VT>(b, sd, slice, threadIdx.x & 31, x + (int64_t)blockIdx.y * ldx,
-                 y + (int64_t)blockIdx.y * ldy, accumulate);
+  sell_slice<VT, PACKED>(b, sd, slice, threadIdx.x & 31, x + (int64_t)blockIdx.y * ldx,
+                         y + (int64_t)blockIdx.y * ldy, accumulate);
 }
 
 int gridn(int64_t n) {
@@ -186,8 +205,12 @@ static edk_status launch_sell(const BasisDev& b, const SellDev& sd, const void* 
   for (int64_t k0 = 0; k0 < nvec; k0 += 65535) {
     int64_t nk = std::min<int64_t>(nvec - k0, 65535);
     dim3 grid((unsigned)((sd.nslices + 7) / 8), (unsigned)nk);
-    k_sell_apply<VT><<<grid, 256, 0, st>>>(b, sd, static_cast<const VT*>(x) + k0 * ldx,
-                                           static_cast<VT*>(y) + k0 * ldy, ldx, ldy, accumulate);
+    const VT* xs = static_cast<const VT*>(x) + k0 * ldx;
+    VT* ys = static_cast<VT*>(y) + k0 * ldy;
+    if (sd.packed)
+      k_sell_apply<VT, 1><<<grid, 256, 0, st>>>(b, sd, xs, ys, ldx, ldy, accumulate);
+    else
+      k_sell_apply<VT, 0><<<grid, 256, 0, st>>>(b, sd, xs, ys, ldx, ldy, accumulate);
     EDK_TRY_CUDA(cudaGetLastError());
   }
   return EDK_OK;
@@ -234,13 +257,20 @@ static edk_status materialize(edk_operator* op) {
   }
   cudaStream_t st = op->stream;
   const int64_t D = b.D;
-  DevBuf cnt;
+  // slot word row | class << rbits: 27 row bits under translations (<= 32
+  // norm classes), 31 otherwise (one class, R = 1)
+  const int rbits = symm ? 27 : 31;
+  if (D >= (int64_t(1) << rbits)) {
+    set_error("edk_operator_materialize: basis dimension too large for the sliced-ELL row index");
+    return EDK_UNSUPPORTED;
+  }
+  DevBuf cnt, drows;
   EDK_RETURN_IF(cnt.alloc(std::max<int64_t>(D, 1)));
-  EDK_RETURN_IF(op->s_diag.alloc(std::max<int64_t>(D, 1) * sizeof(double2)));
+  EDK_RETURN_IF(drows.alloc(std::max<int64_t>(D, 1) * sizeof(double2)));
 #define EDK_CNT(BK)                                                                             \
   case BK:                                                                                      \
     k_sell_count<BK><<<gridn(D), 256, 0, st>>>(b, op->dev, ff, cnt.as<uint8_t>(),              \
-                                               op->s_diag.as<double2>());                      \
+                                               drows.as<double2>());                           \
     break;
   switch (bk) {
     EDK_CNT(BK_TENSOR)
@@ -293,10 +323,15 @@ static edk_status materialize(edk_operator* op) {
                                cudaMemcpyHostToDevice, st));
   EDK_TRY_CUDA(cudaMemcpyAsync(op->s_off.p, off.data(), off.size() * sizeof(int64_t),
                                cudaMemcpyHostToDevice, st));
+  const bool dcx = op->is_complex;
+  EDK_RETURN_IF(op->s_diag.alloc(nslices * 32 * (dcx ? sizeof(double2) : sizeof(double))));
+  double* dre = dcx ? nullptr : op->s_diag.as<double>();
+  double2* dcp = dcx ? op->s_diag.as<double2>() : nullptr;
 #define EDK_FILL(BK)                                                                            \
   case BK:                                                                                      \
     k_sell_fill<BK><<<gridn(nslices * 32), 256, 0, st>>>(                                       \
-        b, ff, nslices, op->s_rowid.as<int>(), op->s_off.as<int64_t>(), op->s_width.as<int>(), \
+        b, ff, nslices, op->s_rowid.as<int>(), drows.as<double2>(), dre, dcp, rbits,           \
+        op->s_off.as<int64_t>(), op->s_width.as<int>(),                                         \
         op->s_col.as<int>(), op->s_code.as<uint16_t>(), nph, ncls, packed);                    \
     break;
   switch (bk) {
@@ -330,6 +365,11 @@ static edk_status materialize(edk_operator* op) {
         vt32[code] = make_float2((float)re, (float)im);
       }
   }
+  std::vector<double> rinv(32, 1.0);
+  for (int c = 0; c < ncls; ++c) rinv[c] = symm ? 1.0 / b.Rcls[c] : 1.0;
+  EDK_RETURN_IF(op->s_rinv.alloc(rinv.size() * sizeof(double)));
+  EDK_TRY_CUDA(cudaMemcpyAsync(op->s_rinv.p, rinv.data(), rinv.size() * sizeof(double),
+                               cudaMemcpyHostToDevice, st));
   EDK_RETURN_IF(op->s_vt64.alloc(vt.size() * sizeof(double2)));
   EDK_RETURN_IF(op->s_vt32.alloc(vt32.size() * sizeof(float2)));
   EDK_TRY_CUDA(cudaMemcpyAsync(op->s_vt64.p, vt.data(), vt.size() * sizeof(double2),
@@ -340,12 +380,15 @@ static edk_status materialize(edk_operator* op) {
   SellDev& sd = op->dev.sell;
   sd.nslices = nslices;
   sd.packed = packed;
-  sd.rowid = op->s_rowid.as<int>();
+  sd.rbits = rbits;
+  sd.rowid = op->s_rowid.as<unsigned>();
   sd.off = op->s_off.as<int64_t>();
   sd.width = op->s_width.as<int>();
   sd.col = op->s_col.as<int>();
   sd.code = op->s_code.as<uint16_t>();
-  sd.diag = op->s_diag.as<double2>();
+  sd.diag = dre;
+  sd.diagc = dcp;
+  sd.rinv = op->s_rinv.as<double>();
   sd.vt64 = op->s_vt64.as<double2>();
   sd.vt32 = op->s_vt32.as<float2>();
   op->sell_entries = E;
@@ -366,6 +409,7 @@ extern "C" edk_status edk_operator_materialize(edk_operator* op, int32_t enable,
     op->dev.sell = SellDev{};
     op->s_rowid.release(); op->s_off.release(); op->s_width.release(); op->s_col.release();
     op->s_code.release(); op->s_diag.release(); op->s_vt64.release(); op->s_vt32.release();
+    op->s_rinv.release();
     op->sell_entries = 0;
     if (entries) *entries = 0;
     return EDK_OK;
