@@ -23,7 +23,8 @@ PREC_FP64, PREC_MIXED = 0, 1
 EXPORTS = [
     "edk_basis_create", "edk_basis_destroy", "edk_basis_dim", "edk_basis_export",
     "edk_basis_index", "edk_basis_index_noalloc", "edk_operator_create", "edk_operator_destroy", "edk_operator_info",
-    "edk_operator_materialize",
+    "edk_operator_materialize", "edk_operator_configure", "edk_operator_autotune",
+    "edk_basis_set_search", "edk_basis_get_search",
     "edk_apply", "edk_apply_async", "edk_lanczos_e0", "edk_krylov_default_opts",
     "edk_krylov_evolve", "edk_batch_lanczos_e0", "edk_tridiag_eigen", "edk_last_error",
     "edk_version",
@@ -82,6 +83,21 @@ class KrylovDiag(C.Structure):
     ]
 
 
+TUNE_MAX = 24
+KERNEL_FAST, KERNEL_GENERIC, KERNEL_MATERIALIZED = 0, 1, 2
+SEARCH_HASH, SEARCH_SORTED = 0, 1
+TUNE_MATERIALIZE = 1
+
+
+class TuneResult(C.Structure):
+    _fields_ = [
+        ("kernel", C.c_int32), ("search", C.c_int32), ("tps", C.c_int32), ("ms", C.c_double),
+        ("ncand", C.c_int32), ("cand_kernel", C.c_int32 * TUNE_MAX),
+        ("cand_search", C.c_int32 * TUNE_MAX), ("cand_tps", C.c_int32 * TUNE_MAX),
+        ("cand_ms", C.c_double * TUNE_MAX),
+    ]
+
+
 _lib = None
 
 
@@ -105,6 +121,10 @@ def load():
         "edk_operator_create": (st, [vp, i32, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]),
         "edk_operator_destroy": (st, [vp]),
         "edk_operator_materialize": (st, [vp, i32, C.POINTER(i64)]),
+        "edk_operator_configure": (st, [vp, i32, i32]),
+        "edk_operator_autotune": (st, [vp, i32, i64, i32, C.POINTER(TuneResult)]),
+        "edk_basis_set_search": (st, [vp, i32]),
+        "edk_basis_get_search": (st, [vp, C.POINTER(i32)]),
         "edk_operator_info": (st, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32),
                                    C.POINTER(i32)]),
         "edk_apply": (st, [vp, i32, vp, vp, i64, i64, i64, i32, i32]),

@@ -76,6 +76,17 @@ class AbstractBasis:
             except Exception:
                 pass
 
+    def set_search(self, strategy):
+        """Index search of a basis with representatives: "hash" (table) or
+        "sorted" (binary search over the ascending representatives, as
+        EDKit's index() does); rows and results are identical."""
+        E.check(E.load().edk_basis_set_search(self._h, {"hash": 0, "sorted": 1}[strategy]))
+
+    def get_search(self):
+        v = C.c_int32()
+        E.check(E.load().edk_basis_get_search(self._h, C.byref(v)))
+        return {0: "hash", 1: "sorted"}[v.value]
+
     # --- AbstractBasis interface (AbstractBasis.jl:95-176) ---
     def size(self, dim=None):
         return (self._D, self._D) if dim is None else (self._D if dim in (1, 2) else 1)

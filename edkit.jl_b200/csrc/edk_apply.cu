@@ -46,12 +46,12 @@ __global__ void __launch_bounds__(256) k_apply(BasisDev b, OpDev op, const VT* _
     gen_row<BK, S, VT, GATHER>(b, op, i, xk, yk, accumulate, s_binom);
 }
 
-template <int BK, class VT>
+template <int BK, class VT, int TPS>
 __global__ void __launch_bounds__(256) k_apply_ff(BasisDev b, OpDev op, FFParams ff,
                                                   const VT* __restrict__ x, VT* __restrict__ y,
                                                   int64_t ldx, int64_t ldy, int accumulate) {
-  ff_tile<BK, VT>(b, op, ff, (int64_t)blockIdx.x * 256, x + (int64_t)blockIdx.y * ldx,
-                  y + (int64_t)blockIdx.y * ldy, accumulate);
+  ff_tile<BK, VT, TPS>(b, op, ff, (int64_t)blockIdx.x * (256 / TPS),
+                       x + (int64_t)blockIdx.y * ldx, y + (int64_t)blockIdx.y * ldy, accumulate);
 }
 
 namespace {
@@ -63,20 +63,21 @@ int apply_grid(int64_t D) {
   return (int)g;
 }
 
-template <class VT>
+template <class VT, int TPS>
 edk_status launch_apply_ff(const BasisDev& b, const OpDev& op, const FFParams& ff, const void* x,
                            void* y, int64_t nvec, int64_t ldx, int64_t ldy, int accumulate,
                            cudaStream_t st) {
   const VT* X = static_cast<const VT*>(x);
   VT* Y = static_cast<VT*>(y);
+  constexpr int RT = 256 / TPS;
   for (int64_t k0 = 0; k0 < nvec; k0 += 65535) {
     int64_t nk = std::min<int64_t>(nvec - k0, 65535);
-    dim3 grid((unsigned)((b.D + 255) / 256), (unsigned)nk);
+    dim3 grid((unsigned)((b.D + RT - 1) / RT), (unsigned)nk);
     const VT* Xk = X + k0 * ldx;
     VT* Yk = Y + k0 * ldy;
 #define EDK_FF(BK)                                                                         \
   case BK:                                                                                 \
-    k_apply_ff<BK, VT><<<grid, 256, 0, st>>>(b, op, ff, Xk, Yk, ldx, ldy, accumulate);     \
+    k_apply_ff<BK, VT, TPS><<<grid, 256, 0, st>>>(b, op, ff, Xk, Yk, ldx, ldy, accumulate); \
     break;
     switch (b.bk) {
       EDK_FF(BK_TENSOR)
@@ -157,12 +158,19 @@ edk_status apply_device(edk_operator* op, int dtype, const void* x, void* y, int
   if (op->sell_ok && !sc) return apply_sell(op, dtype, x, y, nvec, ldx, ldy, accumulate, st);
   if (op->ff_ok && !sc && op->use_ff) {
     const FFParams& ff = *reinterpret_cast<const FFParams*>(op->ff_params.data());
+#define EDK_FF_TPS(VT)                                                                          \
+  switch (op->tps) {                                                                            \
+    case 2: return launch_apply_ff<VT, 2>(b, op->dev, ff, x, y, nvec, ldx, ldy, accumulate, st); \
+    case 4: return launch_apply_ff<VT, 4>(b, op->dev, ff, x, y, nvec, ldx, ldy, accumulate, st); \
+    default: return launch_apply_ff<VT, 1>(b, op->dev, ff, x, y, nvec, ldx, ldy, accumulate, st); \
+  }
     switch (dtype) {
-      case EDK_F64: return launch_apply_ff<double>(b, op->dev, ff, x, y, nvec, ldx, ldy, accumulate, st);
-      case EDK_C128: return launch_apply_ff<double2>(b, op->dev, ff, x, y, nvec, ldx, ldy, accumulate, st);
-      case EDK_F32: return launch_apply_ff<float>(b, op->dev, ff, x, y, nvec, ldx, ldy, accumulate, st);
-      case EDK_C64: return launch_apply_ff<float2>(b, op->dev, ff, x, y, nvec, ldx, ldy, accumulate, st);
+      case EDK_F64: EDK_FF_TPS(double)
+      case EDK_C128: EDK_FF_TPS(double2)
+      case EDK_F32: EDK_FF_TPS(float)
+      case EDK_C64: EDK_FF_TPS(float2)
     }
+#undef EDK_FF_TPS
   }
   switch (dtype) {
     case EDK_F64:

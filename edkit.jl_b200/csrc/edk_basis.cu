@@ -213,6 +213,21 @@ __global__ void k_cls_from_R(const double* R, int64_t D, BasisDev b, uint8_t* cl
   }
 }
 
+// Tables of the sorted-array search: 32-bit keys, the fence (every 32nd key)
+// and a flag raised where the representatives are not strictly ascending.
+__global__ void k_sorted_tables(const uint64_t* I, int64_t D, uint32_t* keys32, uint32_t* fence,
+                                int* unsorted) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < D;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t s = I[i];
+    if (i + 1 < D && !(s < I[i + 1])) *unsorted = 1;
+    if (keys32) {
+      keys32[i] = (uint32_t)s;
+      if ((i & 31) == 0) fence[i >> 5] = (uint32_t)s;
+    }
+  }
+}
+
 __global__ void k_hash_insert32(const uint64_t* I, const uint8_t* cls, int64_t D, int packed,
                                 unsigned long long* tab, uint64_t hmask, int hbits) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < D;
@@ -781,6 +796,70 @@ extern "C" edk_status edk_basis_create(const edk_basis_desc* desc, edk_basis** o
   return EDK_OK;
 }
 
+// Select the index search of a basis with a representative table: the hash
+// table (default) or the two-level binary search over the sorted array.
+extern "C" edk_status edk_basis_set_search(edk_basis* b, int32_t strategy) {
+  EDK_CHECK_ARG(b != nullptr, "edk_basis_set_search: NULL basis");
+  EDK_CHECK_ARG(strategy == EDK_SEARCH_HASH || strategy == EDK_SEARCH_SORTED,
+                "edk_basis_set_search: unknown strategy");
+  std::lock_guard<std::mutex> lk(b->mu);
+  const int bk = b->dev.bk;
+  if (bk == BK_TENSOR || bk == BK_PROJ_RANK) {
+    set_error("edk_basis_set_search: this basis indexes rows directly (tensor product or "
+              "complete fixed-charge sector), there is no representative search to choose");
+    return EDK_UNSUPPORTED;
+  }
+  if (strategy == EDK_SEARCH_HASH) {
+    b->dev.search = 0;
+    return EDK_OK;
+  }
+  if (!b->keys32.p && !b->fence.p && b->D > 0) {
+    cudaStream_t st = b->stream;
+    const bool narrow = b->L <= 32;
+    DevBuf flag;
+    EDK_RETURN_IF(flag.alloc(sizeof(int)));
+    EDK_TRY_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+    const int64_t nf = (b->D + 31) / 32;
+    if (narrow) {
+      EDK_RETURN_IF(b->keys32.alloc(b->D * sizeof(uint32_t)));
+      EDK_RETURN_IF(b->fence.alloc(nf * sizeof(uint32_t)));
+    }
+    k_sorted_tables<<<grid_for(b->D), 256, 0, st>>>(
+        b->I.as<uint64_t>(), b->D, narrow ? b->keys32.as<uint32_t>() : nullptr,
+        narrow ? b->fence.as<uint32_t>() : nullptr, flag.as<int>());
+    EDK_TRY_CUDA(cudaGetLastError());
+    if (b->dev.packed) {
+      EDK_RETURN_IF(b->rcls8.alloc(b->D));
+      if (b->R.p)
+        k_cls_from_R<<<grid_for(b->D), 256, 0, st>>>(b->R.as<double>(), b->D, b->dev,
+                                                      b->rcls8.as<uint8_t>());
+      else
+        EDK_TRY_CUDA(cudaMemsetAsync(b->rcls8.p, 0, b->D, st));
+      EDK_TRY_CUDA(cudaGetLastError());
+    }
+    int unsorted = 0;
+    EDK_TRY_CUDA(cudaMemcpyAsync(&unsorted, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EDK_TRY_CUDA(cudaStreamSynchronize(st));
+    if (unsorted) {
+      b->keys32.release(); b->fence.release(); b->rcls8.release();
+      set_error("edk_basis_set_search: the representatives are not in ascending order");
+      return EDK_INVALID_ARG;
+    }
+    b->dev.keys32 = narrow ? b->keys32.as<uint32_t>() : nullptr;
+    b->dev.fence = narrow ? b->fence.as<uint32_t>() : nullptr;
+    b->dev.nfence = narrow ? nf : 0;
+    b->dev.rcls8 = b->dev.packed ? b->rcls8.as<uint8_t>() : nullptr;
+  }
+  b->dev.search = 1;
+  return EDK_OK;
+}
+
+extern "C" edk_status edk_basis_get_search(const edk_basis* b, int32_t* strategy) {
+  EDK_CHECK_ARG(b != nullptr && strategy != nullptr, "edk_basis_get_search: NULL argument");
+  *strategy = b->dev.search ? EDK_SEARCH_SORTED : EDK_SEARCH_HASH;
+  return EDK_OK;
+}
+
 namespace edk {
 // Host-side guard run before every kernel launch that reads the basis tables:
 // a lookup kind is only launched with the tables it dereferences.
@@ -802,6 +881,10 @@ edk_status check_basis_dev(const BasisDev& b) {
       break;
     default: ok = false;
   }
+  if (ok && b.search && b.bk != BK_TENSOR && b.bk != BK_PROJ_RANK)
+    ok = (b.L <= 32) ? (b.keys32 != nullptr && b.fence != nullptr) : b.I != nullptr;
+  if (ok && b.search && b.packed && b.bk != BK_TENSOR && b.bk != BK_PROJ_RANK)
+    ok = b.rcls8 != nullptr;
   if (b.D > 0 && !ok) {
     set_error("internal: basis tables missing for its lookup kind");
     return EDK_INVALID_ARG;

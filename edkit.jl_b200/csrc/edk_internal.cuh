@@ -159,6 +159,13 @@ struct BasisDev {
   uint64_t hmask;        // slots - 1
   int hbits;             // log2(slots)
   int packed;            // 1: value = row << 5 | class; 0: value = row, R gathered
+  // sorted-array search (edk_basis_set_search): two-level binary search over
+  // the ascending representatives instead of the hash table
+  int search;              // 0: hash table, 1: sorted array
+  const uint32_t* keys32;  // representatives as 32-bit words (L <= 32), else null
+  const uint32_t* fence;   // keys32[32 j]: first level of the search
+  int64_t nfence;
+  const uint8_t* rcls8;    // norm class of each row (packed values), else null
   int nclass;
   double Rcls[kNormClasses];
   // BK_PROJ_RANK
@@ -247,6 +254,7 @@ struct edk_basis {
   int L = 0, A = 1, len = 1, K = -1, P = 1, Kmom = 0;  // Kmom = mod(-k, len)
   int64_t D = 0;
   edk::DevBuf I, R, htab, phase, gens;
+  edk::DevBuf keys32, fence, rcls8;  // sorted-array search tables (built on demand)
   edk::BasisDev dev{};
   std::vector<edk::GenDev> gens_host;
   std::vector<int> gen_order, gen_q;
@@ -272,6 +280,7 @@ struct edk_operator {
   bool is_complex = false;
   bool ff_ok = false;     // flip-flop bond-family fast path applies
   bool use_ff = true;     // callers may switch the fast path off (A/B checks)
+  int tps = 1;            // threads per state of the fast path (1, 2 or 4; autotuned)
   std::vector<unsigned char> ff_params;
   int max_hits = 0;
   int nfam = 0, ngeneric = 0;

@@ -53,8 +53,55 @@ __host__ __device__ __forceinline__ uint64_t hslot32(uint32_t key, int hbits) {
   return hbits == 0 ? 0 : (uint64_t)(hmix32(key) >> (32 - hbits));
 }
 
+// Sorted-array search: the representatives are stored in ascending order, so
+// the row of a key is its position in that array (the binary search of
+// EDKit's index(), src/Basis/ProjectedBasis.jl:71-81 binary_search).  Level one
+// searches every 32nd key (fence), level two the 32 keys of one 128-byte
+// line.  The value returned is encoded like a hash value.
+__device__ __forceinline__ uint32_t sorted_value(const BasisDev& b, int64_t row) {
+  return b.packed ? ((uint32_t)row << 5) | (uint32_t)__ldg(b.rcls8 + row) : (uint32_t)row;
+}
+__device__ __forceinline__ bool sorted_find32(const BasisDev& b, uint32_t key, uint32_t& val) {
+  int64_t n = b.nfence;
+  if (n == 0 || __ldg(b.fence) > key) return false;
+  int64_t lo = 0;  // invariant: fence[lo] <= key, answer in [lo, lo + n)
+  while (n > 1) {
+    const int64_t half = n >> 1;
+    if (__ldg(b.fence + lo + half) <= key) { lo += half; n -= half; }
+    else n = half;
+  }
+  int64_t r = lo * 32;
+  n = b.D - r < 32 ? b.D - r : 32;
+  while (n > 1) {
+    const int64_t half = n >> 1;
+    if (__ldg(b.keys32 + r + half) <= key) { r += half; n -= half; }
+    else n = half;
+  }
+  if (__ldg(b.keys32 + r) != key) return false;
+  val = sorted_value(b, r);
+  return true;
+}
+__device__ __forceinline__ bool sorted_find64(const BasisDev& b, uint64_t key, uint32_t& val) {
+  int64_t n = b.D;
+  if (n == 0 || __ldg(reinterpret_cast<const unsigned long long*>(b.I)) > key) return false;
+  int64_t lo = 0;
+  while (n > 1) {
+    const int64_t half = n >> 1;
+    if (__ldg(reinterpret_cast<const unsigned long long*>(b.I) + lo + half) <= key) {
+      lo += half;
+      n -= half;
+    } else {
+      n = half;
+    }
+  }
+  if (__ldg(reinterpret_cast<const unsigned long long*>(b.I) + lo) != key) return false;
+  val = sorted_value(b, lo);
+  return true;
+}
+
 // 32-bit keys: one 8-byte slot = key << 32 | value, empty = all ones.
 __device__ __forceinline__ bool hash_find(const BasisDev& b, uint32_t key, uint32_t& val) {
+  if (b.search) return sorted_find32(b, key, val);
   const unsigned long long* tab = reinterpret_cast<const unsigned long long*>(b.htab);
   uint64_t slot = hslot32(key, b.hbits);
   for (uint64_t n = 0; n <= b.hmask; ++n) {
@@ -67,6 +114,7 @@ __device__ __forceinline__ bool hash_find(const BasisDev& b, uint32_t key, uint3
 }
 // 64-bit keys: 16-byte slots {key, value}, empty key = all ones.
 __device__ __forceinline__ bool hash_find(const BasisDev& b, uint64_t key, uint32_t& val) {
+  if (b.search) return sorted_find64(b, key, val);
   const ulonglong2* tab = reinterpret_cast<const ulonglong2*>(b.htab);
   uint64_t slot = hmix64(key) & b.hmask;
   for (uint64_t n = 0; n <= b.hmask; ++n) {

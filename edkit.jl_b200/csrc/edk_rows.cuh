@@ -226,13 +226,18 @@ __device__ __forceinline__ void locate2(const BasisDev& b, const uint32_t* s_bin
     p1 = ok1 ? colex_rank(k1, s_binom) : 0;
     p2 = ok2 ? colex_rank(k2, s_binom) : 0;
   } else {
-    const unsigned long long* tab = reinterpret_cast<const unsigned long long*>(b.htab);
-    const uint64_t q1 = first_slot(b, k1), q2 = first_slot(b, k2);
-    const unsigned long long e1 = __ldg(tab + q1);
-    const unsigned long long e2 = two ? __ldg(tab + q2) : ~0ull;
     uint32_t v1 = 0, v2 = 0;
-    ok1 = probe_rest(b, k1, e1, q1, v1);
-    ok2 = two && probe_rest(b, k2, e2, q2, v2);
+    if (b.search) {
+      ok1 = sorted_find32(b, k1, v1);
+      ok2 = two && sorted_find32(b, k2, v2);
+    } else {
+      const unsigned long long* tab = reinterpret_cast<const unsigned long long*>(b.htab);
+      const uint64_t q1 = first_slot(b, k1), q2 = first_slot(b, k2);
+      const unsigned long long e1 = __ldg(tab + q1);
+      const unsigned long long e2 = two ? __ldg(tab + q2) : ~0ull;
+      ok1 = probe_rest(b, k1, e1, q1, v1);
+      ok2 = two && probe_rest(b, k2, e2, q2, v2);
+    }
     if constexpr (BK == BK_PROJ_HASH) {
       p1 = b.packed ? (int64_t)(v1 >> 5) : (int64_t)v1;
       p2 = b.packed ? (int64_t)(v2 >> 5) : (int64_t)v2;
@@ -244,8 +249,12 @@ __device__ __forceinline__ void locate2(const BasisDev& b, const uint32_t* s_bin
   }
 }
 
-// 256 consecutive rows r0.. of the flip-flop fast path (one block).
-template <int BK, class VT>
+// 256 / TPS consecutive rows r0.. of the flip-flop fast path (one block of
+// 256 threads).  Rows are sorted by their number of off-diagonal hits so that
+// the lanes of a warp loop equally long; TPS adjacent lanes share one row and
+// take its pairs of hits in turn (threads per state, picked by the
+// autotuner), then reduce with shuffles.
+template <int BK, class VT, int TPS = 1>
 __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, const FFParams& ff,
                                         int64_t r0, const VT* __restrict__ xk,
                                         VT* __restrict__ yk, int accumulate) {
@@ -256,6 +265,7 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
   __shared__ unsigned short s_order[256];
   __shared__ uint32_t s_state[256];
   if constexpr (BK == BK_PROJ_RANK) fill_binom32(s_binom);
+  constexpr int RT = 256 / TPS;  // rows per tile
   const int t = threadIdx.x;
   if (t < 64) s_hist[t] = 0;
   __syncthreads();
@@ -263,14 +273,17 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
   const int L = b.L;
   uint32_t s = 0;
   int key = 0;
-  if (r0 + t < b.D) {
+  if (t < RT && r0 + t < b.D) {
     s = (BK == BK_TENSOR) ? (uint32_t)(r0 + t) : (uint32_t)__ldg(b.I + r0 + t);
     for (int f = 0; f < ff.nfam; ++f)
       key += __popc((s ^ rotl_L(s, ff.d[f], L, mask)) & ff.valid[f]);
   }
   key = min(key, 63);
-  s_state[t] = s;
-  const int slot = atomicAdd(&s_hist[key], 1);
+  int slot = 0;
+  if (t < RT) {
+    s_state[t] = s;
+    slot = atomicAdd(&s_hist[key], 1);
+  }
   __syncthreads();
   if (t < 32) {  // exclusive scan over the 64 bins
     const int a = s_hist[2 * t], c = s_hist[2 * t + 1];
@@ -285,13 +298,16 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
     s_hist[2 * t + 1] = excl + a;
   }
   __syncthreads();
-  s_order[s_hist[key] + slot] = (unsigned short)t;
+  if (t < RT) s_order[s_hist[key] + slot] = (unsigned short)t;
   __syncthreads();
-  const int tt = s_order[t];
+  const int tt = s_order[t / TPS];
+  const int sub = TPS > 1 ? t % TPS : 0;
   const int64_t i = r0 + tt;
-  if (i >= b.D) return;
-  const uint32_t st = s_state[tt];
-  const A invRi = b.R ? (A)(1.0 / __ldg(b.R + i)) : (A)1;
+  const bool valid = i < b.D;  // the TPS lanes of a row agree
+  if (TPS == 1 && !valid) return;
+  const uint32_t st = s_state[tt];  // 0 past the last row: no hits
+  const A invRi = (b.R && valid) ? (A)(1.0 / __ldg(b.R + i)) : (A)1;
+  int pc = 0;  // pairs of hits seen so far in this row
   double dr = 0.0, di = 0.0;
   A ar = 0, ai = 0;
   auto acc = [&](const HitCtx& c, double rpos, double vr, double vi, Cx<A> xv) {
@@ -321,6 +337,7 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
       const bool two = bits != 0;
       const int p2 = two ? __ffs(bits) - 1 : p1;
       if (two) bits &= bits - 1;
+      if (TPS > 1 && (pc++ % TPS) != sub) continue;
       const int q1 = p1 >= d ? p1 - d : p1 - d + L, q2 = p2 >= d ? p2 - d : p2 - d + L;
       const uint32_t s1 = st ^ (1u << p1) ^ (1u << q1), s2 = st ^ (1u << p2) ^ (1u << q2);
       HitCtx h1, h2;
@@ -337,6 +354,14 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
       if (ok1) acc(h1, rp1, w1.x, w1.y, x1);
       if (ok2) acc(h2, rp2, w2.x, w2.y, x2);
     }
+  }
+  if constexpr (TPS > 1) {
+#pragma unroll
+    for (int o = 1; o < TPS; o <<= 1) {
+      ar += __shfl_xor_sync(0xffffffffu, ar, o);
+      if constexpr (CX) ai += __shfl_xor_sync(0xffffffffu, ai, o);
+    }
+    if (sub != 0 || !valid) return;
   }
   for (int q = 0; q < op.nterm; ++q) {  // diagonal-only terms (fields, zz on other sites)
     const TermDev* T = op.term + q;

@@ -293,6 +293,29 @@ class Operator:
         E.check(E.load().edk_operator_materialize(self._h, 0, None))
         self.materialized = False
 
+    _KERNELS = {"fast": 0, "generic": 1, "materialized": 2}
+
+    def configure_(self, kernel="fast", tps=1):
+        """Pick the matrix-free kernel by hand: "fast" (bond families, `tps`
+        threads per state) or "generic"; both give the same product."""
+        E.check(E.load().edk_operator_configure(self._h, self._KERNELS[kernel], int(tps)))
+
+    def autotune_(self, dtype=None, nvec=1, materialize=False):
+        """Time every admissible kernel / threads-per-state / index-search
+        combination (and the materialised matrix when `materialize`) on this
+        operator and keep the fastest.  Returns the choice and every timing."""
+        dt = dtype if dtype is not None else (E.C128 if self.is_complex else E.F64)
+        r = E.TuneResult()
+        E.check(E.load().edk_operator_autotune(self._h, dt, int(nvec),
+                                                E.TUNE_MATERIALIZE if materialize else 0,
+                                                C.byref(r)))
+        names = {v: k for k, v in self._KERNELS.items()}
+        srch = {0: "hash", 1: "sorted"}
+        self.materialized = r.kernel == E.KERNEL_MATERIALIZED
+        return {"kernel": names[r.kernel], "search": srch[r.search], "tps": r.tps, "ms": r.ms,
+                "candidates": [(names[r.cand_kernel[i]], srch[r.cand_search[i]], r.cand_tps[i],
+                                r.cand_ms[i]) for i in range(r.ncand)]}
+
     def todense(self):
         """Array(opt) — Operator.jl:171-196 (H times the identity, small D only)."""
         D = self.B.size(1)

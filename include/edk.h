@@ -122,6 +122,22 @@ edk_status edk_basis_index(const edk_basis* b, int64_t n, const uint64_t* states
 edk_status edk_basis_index_noalloc(const edk_basis* b, int64_t n, const uint64_t* states,
                                    int64_t* pos, double* coeff);
 
+/* Index search of a basis with a table of representatives (ProjectedBasis
+ * outside complete sectors, TranslationalBasis, TranslationParityBasis,
+ * AbelianBasis): EDK_SEARCH_HASH (default, open-addressing table) or
+ * EDK_SEARCH_SORTED, a two-level binary search over the ascending
+ * representatives — the search EDKit's index() performs (binary_search,
+ * src/Basis/ProjectedBasis.jl:71-81, called from TranslationalBasis.jl:318-325
+ * and AbelianBasis.jl:678-686).  Both give identical rows; the choice is a
+ * speed trade made by edk_operator_autotune.  The strategy belongs to the
+ * basis and so applies to every operator on it.  EDK_UNSUPPORTED for bases
+ * that index rows directly; EDK_INVALID_ARG when the representatives are not
+ * strictly ascending. */
+#define EDK_SEARCH_HASH 0
+#define EDK_SEARCH_SORTED 1
+edk_status edk_basis_set_search(edk_basis* b, int32_t strategy);
+edk_status edk_basis_get_search(const edk_basis* b, int32_t* strategy);
+
 /* Build an operator from merged local terms — operator() Operator.jl:56-78
  * after its site-list merge, trans_inv_operator() Operator.jl:102-108.
  * Term t acts on nsites[t] sites (1-based, concatenated in `sites`) with a
@@ -149,6 +165,36 @@ edk_status edk_operator_info(const edk_operator* op, int32_t* gather, int32_t* i
  * stored entries.  Available for Hermitian operators built from XXZ-type bond
  * families plus diagonal terms on spin-1/2 bases with L <= 32. */
 edk_status edk_operator_materialize(edk_operator* op, int32_t enable, int64_t* entries);
+
+/* Kernel choice of the matrix-free application.  EDK_KERNEL_FAST: the
+ * bond-family kernel (operators whose off-diagonal part is flip-flop bonds),
+ * with `tps` threads (1, 2, 4) sharing each state; EDK_KERNEL_GENERIC: the
+ * row kernel that handles every operator.  Both compute the same product as
+ * EDKit's mul! (Operator.jl:309-328).  No reference counterpart as a call:
+ * EDKit has one CPU kernel. */
+#define EDK_KERNEL_FAST 0
+#define EDK_KERNEL_GENERIC 1
+#define EDK_KERNEL_MATERIALIZED 2
+edk_status edk_operator_configure(edk_operator* op, int32_t kernel, int32_t tps);
+
+/* Autotuner: times every admissible (kernel, threads per state, index
+ * search) combination — and, with EDK_TUNE_MATERIALIZE or when the operator
+ * is already materialised, the materialised matrix — applying the operator to
+ * `nvec` vectors of `dtype`, then installs the fastest (index search on the
+ * basis, kernel and tps on the operator; a materialised matrix is kept only
+ * when it wins).  Allocates two nvec x D work vectors for the duration.  Not
+ * to be called while other calls use the operator or its basis. */
+#define EDK_TUNE_MATERIALIZE 1
+#define EDK_TUNE_MAX 24
+typedef struct {
+  int32_t kernel, search, tps;  /* the choice installed */
+  double ms;                    /* its median time per application */
+  int32_t ncand;                /* candidates timed */
+  int32_t cand_kernel[EDK_TUNE_MAX], cand_search[EDK_TUNE_MAX], cand_tps[EDK_TUNE_MAX];
+  double cand_ms[EDK_TUNE_MAX];
+} edk_tune_result;
+edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int64_t nvec, int32_t flags,
+                                 edk_tune_result* res);
 
 /* y (+)= H x for an nvec-column block — mul!(y, H, x) Operator.jl:309-328
  * (accumulate=1) and H * x Operator.jl:372-394 (accumulate=0).  Synchronous:
