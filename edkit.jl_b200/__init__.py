@@ -5,8 +5,8 @@ The compute path is libedk.so (hand-written CUDA behind the C ABI in
 include/edk.h); this package is the Python mirror of the reference's Julia API.
 """
 from ._lib import EDKError, load as _load
-from .algorithms import (KrylovEvolutionDiagnostics, batch_lanczos_e0, gapratio, lanczos_e0,
-                         meangapratio, productstate, timeevolve, tridiag_eigen)
+from .algorithms import (KrylovEvolutionDiagnostics, batch_lanczos_e0, block_lanczos, gapratio,
+                         lanczos_e0, meangapratio, productstate, timeevolve, tridiag_eigen)
 from .basis import (AbelianBasis, AbstractBasis, ProjectedBasis, TensorBasis,
                     TranslationalBasis, TranslationParityBasis, basis)
 from .operator import Operator, mul, mul_, operator, spin, trans_inv_operator, Ïƒ
@@ -14,8 +14,8 @@ from .operator import Operator, mul, mul_, operator, spin, trans_inv_operator, Ï
 __all__ = [
     "EDKError", "TensorBasis", "ProjectedBasis", "TranslationalBasis", "TranslationParityBasis",
     "AbelianBasis", "AbstractBasis", "basis", "spin", "Ïƒ", "operator", "trans_inv_operator",
-    "Operator", "mul", "mul_", "lanczos_e0", "batch_lanczos_e0", "timeevolve", "tridiag_eigen",
-    "gapratio", "meangapratio", "productstate", "KrylovEvolutionDiagnostics", "version",
+    "Operator", "mul", "mul_", "lanczos_e0", "batch_lanczos_e0", "block_lanczos", "timeevolve",
+    "tridiag_eigen", "gapratio", "meangapratio", "productstate", "KrylovEvolutionDiagnostics", "version",
 ]
 
 

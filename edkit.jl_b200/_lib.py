@@ -24,7 +24,8 @@ EXPORTS = [
     "edk_basis_create", "edk_basis_destroy", "edk_basis_dim", "edk_basis_export",
     "edk_basis_index", "edk_basis_index_noalloc", "edk_operator_create", "edk_operator_destroy", "edk_operator_info",
     "edk_operator_materialize", "edk_operator_configure", "edk_operator_autotune",
-    "edk_basis_set_search", "edk_basis_get_search",
+    "edk_basis_set_search", "edk_basis_get_search", "edk_block_lanczos",
+    "edk_block_lanczos_default_opts",
     "edk_apply", "edk_apply_async", "edk_lanczos_e0", "edk_krylov_default_opts",
     "edk_krylov_evolve", "edk_batch_lanczos_e0", "edk_tridiag_eigen", "edk_last_error",
     "edk_version",
@@ -83,6 +84,21 @@ class KrylovDiag(C.Structure):
     ]
 
 
+class BlockLanczosOpts(C.Structure):
+    _fields_ = [
+        ("block", C.c_int32), ("max_steps", C.c_int32), ("nev", C.c_int32), ("tol", C.c_double),
+        ("check_every", C.c_int32), ("seed", C.c_uint64),
+    ]
+
+
+class BlockLanczosDiag(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int32), ("matvecs", C.c_int64), ("breakdowns", C.c_int32),
+        ("converged", C.c_int32), ("seconds", C.c_double), ("seconds_spmm", C.c_double),
+        ("seconds_orth", C.c_double), ("seconds_eig", C.c_double),
+    ]
+
+
 TUNE_MAX = 24
 KERNEL_FAST, KERNEL_GENERIC, KERNEL_MATERIALIZED = 0, 1, 2
 SEARCH_HASH, SEARCH_SORTED = 0, 1
@@ -124,6 +140,9 @@ def load():
         "edk_operator_configure": (st, [vp, i32, i32]),
         "edk_operator_autotune": (st, [vp, i32, i64, i32, C.POINTER(TuneResult)]),
         "edk_basis_set_search": (st, [vp, i32]),
+        "edk_block_lanczos_default_opts": (None, [C.POINTER(BlockLanczosOpts)]),
+        "edk_block_lanczos": (st, [i32, vp, C.POINTER(BlockLanczosOpts), vp, vp,
+                                   C.POINTER(BlockLanczosDiag)]),
         "edk_basis_get_search": (st, [vp, C.POINTER(i32)]),
         "edk_operator_info": (st, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32),
                                    C.POINTER(i32)]),

@@ -77,6 +77,30 @@ def batch_lanczos_e0(ops, v0s=None, *, m=200, nev=1, tol=0.0, check_every=10, pr
     return ev.reshape(len(ops), nev), _diag_dict(d)
 
 
+def block_lanczos(ops, x0s=None, *, block=64, m=100, nev=4, tol=0.0, check_every=10,
+                  seed=1234):
+    """Block Lanczos over many operators, `block` right-hand sides each.
+
+    Returns (evals[nops, nev], info): the lowest `nev` distinct eigenvalues of
+    every operator.  x0s: per operator a D x block start block (complex), or
+    None for seeded N(0,1) real and imaginary parts drawn on the device."""
+    o = E.BlockLanczosOpts()
+    E.load().edk_block_lanczos_default_opts(C.byref(o))
+    o.block, o.max_steps, o.nev, o.tol, o.check_every, o.seed = block, m, nev, tol, \
+        check_every, seed
+    x = None
+    if x0s is not None:
+        x = np.concatenate([np.asarray(a, np.complex128).ravel(order="F") for a in x0s])
+    hs = (C.c_void_p * len(ops))(*[op._h.value for op in ops])
+    ev = np.zeros(len(ops) * nev)
+    d = E.BlockLanczosDiag()
+    E.check(E.load().edk_block_lanczos(len(ops), hs, C.byref(o),
+                                       E.ptr(x) if x is not None else None, E.ptr(ev),
+                                       C.byref(d)))
+    info = {k: getattr(d, k) for k, _ in E.BlockLanczosDiag._fields_}
+    return ev.reshape(len(ops), nev), info
+
+
 class KrylovEvolutionDiagnostics(dict):
     def __getattr__(self, k):
         return self[k]

@@ -166,6 +166,40 @@ edk_status edk_operator_info(const edk_operator* op, int32_t* gather, int32_t* i
  * families plus diagonal terms on spin-1/2 bases with L <= 32. */
 edk_status edk_operator_materialize(edk_operator* op, int32_t enable, int64_t* entries);
 
+/* Block Lanczos over a batch of operators (e.g. the momentum sectors of one
+ * chain), each with a block of `block` right-hand-side vectors: the block
+ * form of EDKit's Lanczos recurrence (_lanczos_build!,
+ * src/algorithms/TimeEvolution.jl:250-306) with two classical block
+ * Gram-Schmidt passes against the two previous blocks and Cholesky-QR
+ * (twice) for the next block.  The lowest `nev` distinct eigenvalues of each
+ * operator's block-tridiagonal matrix are returned in evals[q * nev + k]
+ * (NaN where fewer exist).  x0: per operator a D_q x block column-major
+ * complex128 start block (host), concatenated; NULL draws seeded N(0,1) real
+ * and imaginary parts on the device from opts->seed.  Every operator must be
+ * Hermitian in the row-gather form and block * max_steps below its dimension.
+ * tol > 0 stops when every operator's nev values move less than
+ * tol * max(1, |E0|) between checks (every check_every steps); tol = 0 runs
+ * max_steps.  No reference counterpart (EDKit runs one vector). */
+typedef struct {
+  int32_t block;        /* vectors per operator: multiple of 8, 8..64 */
+  int32_t max_steps;    /* block steps */
+  int32_t nev;
+  double tol;
+  int32_t check_every;
+  uint64_t seed;
+} edk_block_lanczos_opts;
+typedef struct {
+  int32_t steps;        /* block steps taken */
+  int64_t matvecs;      /* single-vector products: steps * block * nops */
+  int32_t breakdowns;   /* operators whose Krylov space closed early */
+  int32_t converged;    /* 1 when tol stopped the run */
+  double seconds, seconds_spmm, seconds_orth, seconds_eig;
+} edk_block_lanczos_diag;
+void edk_block_lanczos_default_opts(edk_block_lanczos_opts* opts);
+edk_status edk_block_lanczos(int32_t nops, edk_operator* const* ops,
+                             const edk_block_lanczos_opts* opts, const double* x0, double* evals,
+                             edk_block_lanczos_diag* diag);
+
 /* Kernel choice of the matrix-free application.  EDK_KERNEL_FAST: the
  * bond-family kernel (operators whose off-diagonal part is flip-flop bonds),
  * with `tps` threads (1, 2, 4) sharing each state; EDK_KERNEL_GENERIC: the
