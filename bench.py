@@ -326,9 +326,9 @@ def time_to_e0(ek, H, D):
 
 def config5_ensemble(ek, n_inst=512, seed=2024, steps=200):
     """512 random-field XXZ chains (open, Delta=1, h_i ~ U[-3,3] on spin-1/2 z),
-    L drawn from {12,14,16,18,20}, ProjectedBasis N=L/2: E0 and the gap ratio of
-    the four lowest Ritz values per instance, FP64 batched vs mixed batched, and
-    FP64 one instance at a time on a sample."""
+    L drawn from {12,14,16,18,20}, ProjectedBasis N=L/2.  Time to E0 (nev=1)
+    and to the four lowest levels (nev=4, for the gap ratio): FP64 batched,
+    mixed batched, and FP64 one instance at a time (estimated from a sample)."""
     rng = np.random.default_rng(seed)
     bond = ek.spin((1.0, "xx"), (1.0, "yy"), (1.0, "zz"))
     ops = []
@@ -341,25 +341,30 @@ def config5_ensemble(ek, n_inst=512, seed=2024, steps=200):
     rows = sum(op.size(1) for op in ops)
     v0s = [np.random.default_rng(q).standard_normal(op.size(1)) for q, op in enumerate(ops)]
     res = {"instances": n_inst, "rows": rows}
-    for name, kw in (("fp64_batched", {}), ("mixed_batched", {"precision": "mixed"})):
-        for _ in range(2):
-            ev, d = ek.batch_lanczos_e0(ops, v0s, m=steps, nev=4, tol=1e-12, check_every=10, **kw)
-        res[name] = {"seconds": round(d["seconds"], 4), "max_steps": d["steps"],
-                     "matvecs": d["matvecs"]}
-        res[name + "_E0"] = ev[:, 0]
-    res["dE0_rel_max_mixed_vs_fp64"] = float(np.max(
-        np.abs(res["mixed_batched_E0"] - res["fp64_batched_E0"]) / np.abs(res["fp64_batched_E0"])))
-    res["mean_gap_ratio_low4"] = float(np.mean([np.mean(ek.gapratio(e)) for e in ev]))
-    ns = 32
-    t = time.perf_counter()
-    for q in range(ns):
-        ek.lanczos_e0(ops[q], v0s[q], m=steps, nev=4, tol=1e-12, check_every=10)
-    seq = (time.perf_counter() - t) * n_inst / ns
-    res["fp64_one_at_a_time_seconds_est"] = round(seq, 3)
-    res["speedup_mixed_batched_vs_fp64_one_at_a_time"] = round(seq / res["mixed_batched"]["seconds"], 2)
-    res["speedup_mixed_batched_vs_fp64_batched"] = round(
-        res["fp64_batched"]["seconds"] / res["mixed_batched"]["seconds"], 3)
-    del res["mixed_batched_E0"], res["fp64_batched_E0"]
+    for nev in (1, 4):
+        r, ev = {}, {}
+        for name, kw in (("fp64_batched", {}), ("mixed_batched", {"precision": "mixed"})):
+            for _ in range(2):
+                ev[name], d = ek.batch_lanczos_e0(ops, v0s, m=steps, nev=nev, tol=1e-12,
+                                                  check_every=10, **kw)
+            r[name] = {"seconds": round(d["seconds"], 4), "max_steps": d["steps"],
+                       "matvecs": d["matvecs"]}
+        a, b = ev["fp64_batched"], ev["mixed_batched"]
+        r["dE0_rel_max_mixed_vs_fp64"] = float(np.max(np.abs(b[:, 0] - a[:, 0]) / np.abs(a[:, 0])))
+        r["dE_rel_max_all_levels_mixed_vs_fp64"] = float(np.max(np.abs(b - a) / np.abs(a[:, :1])))
+        ns = 32
+        t = time.perf_counter()
+        for q in range(ns):
+            ek.lanczos_e0(ops[q], v0s[q], m=steps, nev=nev, tol=1e-12, check_every=10)
+        seq = (time.perf_counter() - t) * n_inst / ns
+        r["fp64_one_at_a_time_seconds_est"] = round(seq, 3)
+        r["speedup_mixed_batched_vs_fp64_one_at_a_time"] = round(seq / r["mixed_batched"]["seconds"], 2)
+        r["speedup_mixed_batched_vs_fp64_batched"] = round(
+            r["fp64_batched"]["seconds"] / r["mixed_batched"]["seconds"], 3)
+        if nev == 4:
+            r["mean_gap_ratio_low4_fp64"] = float(np.mean([np.mean(ek.gapratio(e)) for e in a]))
+            r["mean_gap_ratio_low4_mixed"] = float(np.mean([np.mean(ek.gapratio(e)) for e in b]))
+        res["E0_nev1" if nev == 1 else "low4_nev4"] = r
     return res
 
 
@@ -369,40 +374,84 @@ def config4_sectors(ek, steps=100):
     bond = ek.spin((1.0, "xx"), (1.0, "yy"), (1.5, "zz"))
     ops = [ek.trans_inv_operator(bond, 2, ek.TranslationalBasis(L=26, N=13, k=k)) for k in range(26)]
     res = {"sectors": 26, "dims": [op.size(1) for op in ops]}
+    low = {}
     for name, kw in (("fp64_batched", {}), ("mixed_batched", {"precision": "mixed"})):
         for _ in range(2):
-            ev, d = ek.batch_lanczos_e0(ops, m=steps, nev=4, tol=1e-12, check_every=10, **kw)
+            ev, d = ek.batch_lanczos_e0(ops, m=300, nev=4, tol=1e-12, check_every=10, **kw)
         res[name] = {"seconds": round(d["seconds"], 4), "max_steps": d["steps"]}
         res[name + "_low4_k0"] = [float(v) for v in ev[0]]
+        low[name] = ev
     res["E0_all_sectors"] = float(np.min(ev[:, 0]))
+    res["dE_rel_max_mixed_vs_fp64_low4"] = float(np.max(
+        np.abs(low["mixed_batched"] - low["fp64_batched"]) / np.abs(low["fp64_batched"][:, :1])))
+    # the block form: 64 seeded N(0,1) right-hand sides per sector, 100 block steps
+    evb, db = ek.block_lanczos(ops, block=64, m=steps, nev=4, check_every=0, seed=2026)
+    res["block64_lanczos"] = {k: (round(v, 4) if isinstance(v, float) else v)
+                              for k, v in db.items()}
+    res["block64_lanczos"]["dE_rel_max_vs_single_vector_fp64"] = float(np.max(
+        np.abs(evb - low["fp64_batched"]) / np.abs(low["fp64_batched"][:, :1])))
     return res
 
 
 def config3_krylov(ek, ntimes=101):
     """J1-J2 XXZ L=32 (J2=0.5), N=16, k=0 (D=18,784,170): Krylov exp(-iHt) psi0
-    from a seeded random product state, t = 0..10 step 0.1, m = 30; FP32 complex
-    Krylov vectors (mixed) vs FP64: fidelity and energy drift at the last time."""
+    from a seeded random product state at t = 0, 0.1, ..., 10 (all 101 states
+    kept in HBM), m = 30.  FP32 complex Krylov vectors (mixed) against the FP64
+    run: worst fidelity and energy drift over the trajectory; both again on the
+    materialised operator."""
+    import torch
+    from edkit_b200 import _lib as E
     b = ek.TranslationalBasis(L=32, N=16, k=0)
     H = ek.trans_inv_operator(ek.spin((1.0, "xx"), (1.0, "yy"), (1.0, "zz")), 2, b) + \
         ek.trans_inv_operator(ek.spin((0.5, "xx"), (0.5, "yy"), (0.5, "zz")), [1, 3], b)
     rng = np.random.default_rng(99)
     dg = np.zeros(32, dtype=np.int64)
     dg[rng.choice(32, 16, replace=False)] = 1
-    psi0 = ek.productstate(dg, b).astype(np.complex128)
+    psi0 = torch.from_numpy(ek.productstate(dg, b).astype(np.complex128)).cuda()
     ts = np.round(np.arange(ntimes) * 0.1, 10)
-    res = {"D": b.size(1), "times": len(ts)}
-    out = {}
-    for name, prec in (("fp64", "fp64"), ("mixed", "mixed")):
-        psi, d = ek.timeevolve(H, psi0, ts[-1:], tol=1e-10, m_init=30, m_max=30,
+    D = b.size(1)
+    res = {"D": D, "times": len(ts)}
+    lib = E.load()
+    y = torch.empty(D, dtype=torch.complex128, device="cuda")
+
+    def energy(v):
+        E.check(lib.edk_apply(H._h, E.C128, E.ptr(v), E.ptr(y), 1, D, D, 0, E.DEVICE))
+        return float(torch.vdot(v, y).real / torch.vdot(v, v).real)
+
+    def run(prec):
+        psi, d = ek.timeevolve(H, psi0, ts, tol=1e-10, m_init=30, m_max=30,
                                return_diagnostics=True, precision=prec)
-        res[name] = {"seconds": round(d.seconds, 3), "matvecs": d.matvecs,
+        return psi, {"seconds": round(d.seconds, 3), "matvecs": d.matvecs,
                      "restarts": d.restarts}
-        out[name] = psi[:, 0]
-    a, m = out["fp64"], out["mixed"]
-    res["fidelity_t10"] = float(abs(np.vdot(a, m)) ** 2 / (np.vdot(a, a).real * np.vdot(m, m).real))
-    e0 = float(np.vdot(psi0, H * psi0).real)
-    res["energy_drift_fp64"] = float(np.vdot(a, H * a).real / np.vdot(a, a).real - e0)
-    res["energy_drift_mixed"] = float(np.vdot(m, H * m).real / np.vdot(m, m).real - e0)
+
+    def compare(a, m):
+        fid = []
+        for q in range(a.shape[1]):
+            x, z = a[:, q], m[:, q]
+            fid.append(float(torch.vdot(x, z).abs() ** 2 /
+                             (torch.vdot(x, x).real * torch.vdot(z, z).real)))
+        return 1.0 - min(fid)
+
+    e_init = energy(psi0)
+    ref, res["fp64"] = run("fp64")
+    mix, res["mixed"] = run("mixed")
+    res["max_infidelity_mixed_vs_fp64"] = compare(ref, mix)
+    res["max_energy_drift_fp64"] = max(abs(energy(ref[:, q].contiguous()) - e_init)
+                                       for q in range(0, len(ts), 10))
+    res["max_energy_drift_mixed"] = max(abs(energy(mix[:, q].contiguous()) - e_init)
+                                        for q in range(0, len(ts), 10))
+    del mix
+    torch.cuda.empty_cache()
+    t = time.perf_counter()
+    entries = H.sparse_()
+    res["materialized_build_seconds"] = round(time.perf_counter() - t, 3)
+    res["materialized_entries"] = entries
+    for prec in ("fp64", "mixed"):
+        st, res[prec + "_materialized"] = run(prec)
+        res[prec + "_materialized"]["max_infidelity_vs_fp64_matrix_free"] = compare(ref, st)
+        del st
+        torch.cuda.empty_cache()
+    H.clear_sparse_cache_()
     return res
 
 

@@ -117,8 +117,13 @@ def timeevolve(H: Operator, psi0, t, *, return_diagnostics=False, tol=1e-10, m_i
     if np.any(ts < 0):
         raise ValueError("timeevolve: all times in ts must be non-negative; backward evolution "
                          "is not supported")
-    psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
     D = H.size(1)
+    on_device = hasattr(psi0, "data_ptr") and getattr(psi0, "is_cuda", False)
+    if on_device:
+        import torch
+        psi0 = psi0.to(torch.complex128).contiguous()
+    else:
+        psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
     if psi0.shape[0] != D:
         raise ValueError("psi0 has the wrong length")
     o = E.KrylovOpts()
@@ -128,10 +133,16 @@ def timeevolve(H: Operator, psi0, t, *, return_diagnostics=False, tol=1e-10, m_i
     o.reuse_basis, o.extend_basis = int(reuse_basis), int(extend_basis)
     o.normalize_output = int(normalize_output)
     o.precision = {"fp64": E.PREC_FP64, "mixed": E.PREC_MIXED}[precision]
-    out = np.zeros((D, len(ts)), dtype=np.complex128, order="F")
+    if on_device:  # states stay in HBM: column q of the (D, nts) view is time ts[q]
+        out = torch.empty((len(ts), D), dtype=torch.complex128, device=psi0.device)
+    else:
+        out = np.zeros((D, len(ts)), dtype=np.complex128, order="F")
     d = E.KrylovDiag()
     E.check(E.load().edk_krylov_evolve(H._h, C.byref(o), E.ptr(psi0), E.ptr(ts), len(ts),
-                                       E.ptr(out), E.HOST, C.byref(d)))
+                                       E.ptr(out), E.DEVICE if on_device else E.HOST,
+                                       C.byref(d)))
+    if on_device:
+        out = out.t()
     diag = KrylovEvolutionDiagnostics(
         basis_builds=d.basis_builds, basis_extensions=d.basis_extensions, restarts=d.restarts,
         matvecs=d.matvecs, total_times_served=d.total_times_served, max_dim_used=d.max_dim_used,

@@ -831,33 +831,66 @@ edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczo
   int steps_low = 0, mvs = 0, bd = 0;
   for (auto& r : res) { steps_low = std::max(steps_low, r.steps); mvs += r.steps; bd |= r.status == 2; }
   if (mixed) {
-    // FP64 refinement rounds restarted from the Ritz vectors
-    int mr = o.refine_steps > 0 ? o.refine_steps : 20;
-    if (o.nev > 1) mr = std::max(mr, 15 * o.nev);
+    // FP64 refinement restarted from the sum of the nev lowest Ritz vectors.
+    // A single eigenvalue converges in a few steps from its FP32 Ritz vector;
+    // several need room to separate close levels, so the round may run to
+    // max_steps (each operator stops when it converges).  Operators that
+    // reach the step limit without converging are restarted again, alone.
+    const int mr = o.nev > 1 ? std::max(o.max_steps, o.refine_steps)
+                             : (o.refine_steps > 0 ? o.refine_steps : 20);
+    std::vector<int> active(nops);
+    for (int q = 0; q < nops; ++q) active[q] = q;
+    DevBuf cur;  // start vectors of `active`, compact in that order
     EDK_RETURN_IF(ritz_vectors(E, res, start.p, o.nev));
-    for (int round = 0; round < 8; ++round) {
+    void* cur_p = start.p;
+    for (int round = 0; round < 4 && !active.empty(); ++round) {
+      std::vector<edk_operator*> sub;
+      for (int q : active) sub.push_back(ops[q]);
       BatchEngine F;
-      EDK_RETURN_IF(F.init(ops, wdt, mr, bk, ff, st));
-      EDK_RETURN_IF(F.setup(start.p));
+      EDK_RETURN_IF(F.init(sub, wdt, mr, bk, ff, st));
+      EDK_RETURN_IF(F.setup(cur_p));
       std::vector<OpResult> r2;
       ++rounds;
       EDK_RETURN_IF(run_batch(F, mr, o.nev, o.tol, std::min(5, mr), r2, &nchecks));
-      // a round is final when every operator converged (or broke down) inside
-      // it, or when it no longer moved the lowest Ritz value
-      bool done = true;
-      for (int q = 0; q < nops; ++q) {
-        bool inside = r2[q].status == 1 || r2[q].status == 2;
-        bool still = r2[q].ev.size() == res[q].ev.size();
-        for (size_t k = 0; k < r2[q].ev.size() && still; ++k) {
-          const double a = r2[q].ev[k], b = res[q].ev[k];
+      std::vector<int> next;
+      std::vector<int> keep;  // positions in `active` of the operators to restart
+      for (size_t i = 0; i < active.size(); ++i) {
+        const int q = active[i];
+        bool still = r2[i].ev.size() == res[q].ev.size();
+        for (size_t k = 0; k < r2[i].ev.size() && still; ++k) {
+          const double a = r2[i].ev[k], b = res[q].ev[k];
           still = std::fabs(a - b) <= std::max(o.tol, 1e-14) * std::max(1.0, std::fabs(a));
         }
-        if (!(inside || still)) done = false;
-        mvs += r2[q].steps;
+        mvs += r2[i].steps;
+        res[q] = r2[i];
+        if (r2[i].status == 0 && !still && o.tol > 0) {
+          next.push_back(q);
+          keep.push_back((int)i);
+        }
       }
-      res = r2;
-      if (done || o.tol <= 0) break;
-      EDK_RETURN_IF(ritz_vectors(F, res, start.p, o.nev));
+      if (next.empty()) break;
+      // Ritz vectors of this round (F's layout), then the restarted subset
+      DevBuf full;
+      EDK_RETURN_IF(full.alloc_async((size_t)F.totalD * esz(wdt), st));
+      EDK_RETURN_IF(ritz_vectors(F, r2, full.p, o.nev));
+      int64_t tot = 0;
+      for (int i : keep) tot += F.Ds[i];
+      DevBuf nb;
+      EDK_RETURN_IF(nb.alloc_async((size_t)std::max<int64_t>(tot, 1) * esz(wdt), st));
+      int64_t dst = 0;
+      for (int i : keep) {
+        EDK_TRY_CUDA(cudaMemcpyAsync((char*)nb.p + dst * esz(wdt),
+                                     (char*)full.p + F.hops[i].woff * esz(wdt),
+                                     (size_t)F.Ds[i] * esz(wdt), cudaMemcpyDeviceToDevice, st));
+        dst += F.Ds[i];
+      }
+      EDK_TRY_CUDA(cudaStreamSynchronize(st));
+      std::swap(cur.p, nb.p);
+      std::swap(cur.bytes, nb.bytes);
+      std::swap(cur.pooled, nb.pooled);
+      std::swap(cur.pool_stream, nb.pool_stream);
+      cur_p = cur.p;
+      active = next;
     }
   }
   EDK_TRY_CUDA(cudaStreamSynchronize(st));

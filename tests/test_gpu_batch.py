@@ -118,3 +118,23 @@ def test_materialized_batch_and_krylov(ek, O):
     H.clear_sparse_cache_()
     b_ = ek.timeevolve(H, psi0, [0.5, 2.0], tol=1e-11)
     assert np.linalg.norm(a - b_) < 1e-9
+
+
+def test_mixed_ensemble_all_four_levels(ek, O):
+    """Every one of the four lowest levels of a disorder ensemble (some with
+    close levels) from the mixed path matches the FP64 batched path and, for
+    the small chains, the dense spectrum."""
+    rng = np.random.default_rng(2024)
+    ops, dense = [], []
+    for q in range(24):
+        L = (10, 12, 14)[q % 3]
+        H, Ho = random_field_instance(ek, O, L, rng)
+        ops.append(H)
+        dense.append(np.linalg.eigvalsh(Ho.dense())[:4] if L <= 12 else None)
+    e64, _ = ek.batch_lanczos_e0(ops, m=200, nev=4, tol=1e-12, check_every=10)
+    emx, info = ek.batch_lanczos_e0(ops, m=200, nev=4, tol=1e-12, check_every=10,
+                                    precision="mixed")
+    for q in range(len(ops)):
+        assert np.allclose(emx[q], e64[q], rtol=0, atol=1e-9 * abs(e64[q][0])), q
+        if dense[q] is not None:
+            assert np.allclose(e64[q], dense[q], rtol=0, atol=1e-9 * abs(dense[q][0])), q
