@@ -21,7 +21,7 @@ using EDKit, LinearAlgebra, SparseArrays
 import Base: *, size, eltype
 import LinearAlgebra: mul!
 
-export B200Operator, lanczos_e0, timeevolve
+export B200Operator, lanczos_e0, timeevolve, autotune!, block_lanczos
 
 const libedk = get(ENV, "EDK_LIB", joinpath(@__DIR__, "..", "libedk.so"))
 
@@ -203,6 +203,67 @@ function timeevolve(H::B200Operator, ψ0::AbstractVector, ts::AbstractVector{<:R
          Int32, Ref{KrylovDiag}), H.h, o, ψ, t, length(t), out, 0, d))
     return_diagnostics ? (out, d) : out
 end
+# sparse!(opt) / clear_sparse_cache! (Operator.jl:221-285) on the device
+function EDKit.sparse!(H::B200Operator)
+    n = Ref{Int64}(0)
+    check(ccall((:edk_operator_materialize, libedk), Cint, (Ptr{Cvoid}, Int32, Ref{Int64}),
+                H.h, 1, n))
+    n[]
+end
+clear_sparse!(H::B200Operator) =
+    check(ccall((:edk_operator_materialize, libedk), Cint, (Ptr{Cvoid}, Int32, Ptr{Int64}),
+                H.h, 0, C_NULL))
+
+struct TuneResult
+    kernel::Int32; search::Int32; tps::Int32; ms::Float64; ncand::Int32
+    cand_kernel::NTuple{24, Int32}; cand_search::NTuple{24, Int32}; cand_tps::NTuple{24, Int32}
+    cand_ms::NTuple{24, Float64}
+end
+
+"""
+    autotune!(H::B200Operator, T=Float64; nvec=1, materialize=false)
+
+Time every kernel / threads-per-state / index-search choice (and the
+materialised matrix with `materialize=true`) on H and keep the fastest.
+"""
+function autotune!(H::B200Operator, ::Type{T}=Float64; nvec::Integer=1,
+                   materialize::Bool=false) where T
+    r = Ref{TuneResult}()
+    check(ccall((:edk_operator_autotune, libedk), Cint,
+                (Ptr{Cvoid}, Int32, Int64, Int32, Ref{TuneResult}),
+                H.h, dtype_code(T), nvec, materialize ? 1 : 0, r))
+    r[]
+end
+
+struct BlockLanczosOpts
+    block::Int32; max_steps::Int32; nev::Int32; tol::Float64; check_every::Int32; seed::UInt64
+end
+mutable struct BlockLanczosDiag
+    steps::Int32; matvecs::Int64; breakdowns::Int32; converged::Int32
+    seconds::Float64; seconds_spmm::Float64; seconds_orth::Float64; seconds_eig::Float64
+    BlockLanczosDiag() = new(0, 0, 0, 0, 0.0, 0.0, 0.0, 0.0)
+end
+
+"""
+    block_lanczos(Hs::Vector{<:B200Operator}; block=64, m=100, nev=4, tol=0.0, seed=1234)
+
+Block Lanczos over all operators at once (e.g. every momentum sector), `block`
+seeded random right-hand sides each; returns an nev x length(Hs) matrix of the
+lowest distinct eigenvalues.
+"""
+function block_lanczos(Hs::AbstractVector{<:B200Operator}; block::Integer=64, m::Integer=100,
+                       nev::Integer=4, tol::Real=0.0, check_every::Integer=10,
+                       seed::Integer=1234)
+    hs = Ptr{Cvoid}[H.h for H in Hs]
+    o = BlockLanczosOpts(block, m, nev, tol, check_every, seed)
+    ev = zeros(nev, length(Hs))
+    d = BlockLanczosDiag()
+    GC.@preserve hs ev check(ccall((:edk_block_lanczos, libedk), Cint,
+        (Int32, Ptr{Ptr{Cvoid}}, Ref{BlockLanczosOpts}, Ptr{Float64}, Ptr{Float64},
+         Ref{BlockLanczosDiag}), length(Hs), hs, o, C_NULL, ev, d))
+    ev, d
+end
+
 timeevolve(H::B200Operator, ψ0::AbstractVector, t::Real; kw...) =
     (t < 0 && error("timeevolve!: requested time $t precedes anchor time 0.0");
      timeevolve(H, ψ0, [t]; kw...)[:, 1])
