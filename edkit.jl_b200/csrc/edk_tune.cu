@@ -114,8 +114,8 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
   if ((flags & EDK_TUNE_MATERIALIZE) || was_mat) cands.push_back({EDK_KERNEL_MATERIALIZED, 0, 1});
 
   const int reps = 7;
-  double best = 1e300;
-  Cand pick = cands.front();
+  double best = 1e300, best_free = 1e300;
+  Cand pick = cands.front(), pick_free = cands.front();
   edk_status rc = EDK_OK;
   for (const Cand& c : cands) {
     double ms = -1.0;
@@ -140,20 +140,19 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
       ++out.ncand;
     }
     if (ms < best) { best = ms; pick = c; }
+    if (c.kernel != EDK_KERNEL_MATERIALIZED && ms < best_free) { best_free = ms; pick_free = c; }
   }
   if (rc != EDK_OK) return rc;
-  // install the fastest
-  if (pick.kernel == EDK_KERNEL_MATERIALIZED) {
-    EDK_RETURN_IF(edk_operator_materialize(op, 1, nullptr));
-  } else {
-    if (op->sell_ok) edk_operator_materialize(op, 0, nullptr);
-    if (has_search) edk_basis_set_search(b, pick.search);
-    op->use_ff = pick.kernel == EDK_KERNEL_FAST;
-    op->tps = pick.tps;
-  }
+  // install the fastest matrix-free choice (it also serves whenever the
+  // materialised matrix is cleared), then the matrix if that wins
+  if (op->sell_ok && pick.kernel != EDK_KERNEL_MATERIALIZED) edk_operator_materialize(op, 0, nullptr);
+  if (has_search) edk_basis_set_search(b, pick_free.search);
+  op->use_ff = pick_free.kernel == EDK_KERNEL_FAST;
+  op->tps = pick_free.tps;
+  if (pick.kernel == EDK_KERNEL_MATERIALIZED) EDK_RETURN_IF(edk_operator_materialize(op, 1, nullptr));
   out.kernel = pick.kernel;
   out.search = b->dev.search ? EDK_SEARCH_SORTED : EDK_SEARCH_HASH;
-  out.tps = pick.tps;
+  out.tps = pick_free.tps;
   out.ms = best;
   if (res) *res = out;
   return EDK_OK;

@@ -214,9 +214,9 @@ edk_status edk_operator_configure(edk_operator* op, int32_t kernel, int32_t tps)
 /* Autotuner: times every admissible (kernel, threads per state, index
  * search) combination — and, with EDK_TUNE_MATERIALIZE or when the operator
  * is already materialised, the materialised matrix — applying the operator to
- * `nvec` vectors of `dtype`, then installs the fastest (index search on the
- * basis, kernel and tps on the operator; a materialised matrix is kept only
- * when it wins).  Allocates two nvec x D work vectors for the duration.  Not
+ * `nvec` vectors of `dtype`, then installs the fastest matrix-free choice
+ * (index search on the basis, kernel and tps on the operator) and, when it
+ * wins, the materialised matrix on top (kept only then).  Allocates two nvec x D work vectors for the duration.  Not
  * to be called while other calls use the operator or its basis. */
 #define EDK_TUNE_MATERIALIZE 1
 #define EDK_TUNE_MAX 24
