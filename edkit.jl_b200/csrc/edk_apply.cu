@@ -49,8 +49,9 @@ __global__ void __launch_bounds__(256) k_apply(BasisDev b, OpDev op, const VT* _
 template <int BK, class VT, int TPS>
 __global__ void __launch_bounds__(256) k_apply_ff(BasisDev b, OpDev op, FFParams ff,
                                                   const VT* __restrict__ x, VT* __restrict__ y,
-                                                  int64_t ldx, int64_t ldy, int accumulate) {
-  ff_tile<BK, VT, TPS>(b, op, ff, (int64_t)blockIdx.x * (256 / TPS),
+                                                  int64_t ldx, int64_t ldy, int accumulate,
+                                                  int64_t tile0) {
+  ff_tile<BK, VT, TPS>(b, op, ff, (tile0 + blockIdx.x) * (256 / TPS),
                        x + (int64_t)blockIdx.y * ldx, y + (int64_t)blockIdx.y * ldy, accumulate);
 }
 
@@ -66,18 +67,22 @@ int apply_grid(int64_t D) {
 template <class VT, int TPS>
 edk_status launch_apply_ff(const BasisDev& b, const OpDev& op, const FFParams& ff, const void* x,
                            void* y, int64_t nvec, int64_t ldx, int64_t ldy, int accumulate,
-                           cudaStream_t st) {
+                           cudaStream_t st, int64_t row0 = 0, int64_t row1 = -1) {
   const VT* X = static_cast<const VT*>(x);
   VT* Y = static_cast<VT*>(y);
   constexpr int RT = 256 / TPS;
+  if (row1 < 0) row1 = b.D;
+  const int64_t tile0 = row0 / RT, tile1 = (row1 + RT - 1) / RT;
+  if (tile1 <= tile0) return EDK_OK;
   for (int64_t k0 = 0; k0 < nvec; k0 += 65535) {
     int64_t nk = std::min<int64_t>(nvec - k0, 65535);
-    dim3 grid((unsigned)((b.D + RT - 1) / RT), (unsigned)nk);
+    dim3 grid((unsigned)(tile1 - tile0), (unsigned)nk);
     const VT* Xk = X + k0 * ldx;
     VT* Yk = Y + k0 * ldy;
 #define EDK_FF(BK)                                                                         \
   case BK:                                                                                 \
-    k_apply_ff<BK, VT, TPS><<<grid, 256, 0, st>>>(b, op, ff, Xk, Yk, ldx, ldy, accumulate); \
+    k_apply_ff<BK, VT, TPS><<<grid, 256, 0, st>>>(b, op, ff, Xk, Yk, ldx, ldy, accumulate, \
+                                                  tile0);                                     \
     break;
     switch (b.bk) {
       EDK_FF(BK_TENSOR)
@@ -310,8 +315,46 @@ bool invariant(const std::vector<HostTerm>& terms, const std::vector<int>& perm,
 using namespace edk;
 
 edk_operator::~edk_operator() {
+  for (cudaEvent_t e : cevents) cudaEventDestroy(e);
+  if (cstream) cudaStreamDestroy(cstream);
   if (stream) cudaStreamDestroy(stream);
 }
+
+namespace edk {
+
+bool rows_apply_ok(const edk_operator* op) {
+  if (!op->gather) return false;
+  return op->sell_ok || (op->ff_ok && op->use_ff);
+}
+
+edk_status apply_rows(edk_operator* op, int dtype, const void* x, void* y, int64_t row0,
+                      int64_t row1, int accumulate, cudaStream_t st) {
+  const BasisDev& b = op->b->dev;
+  EDK_RETURN_IF(check_basis_dev(b));
+  if (op->sell_ok) return apply_sell_rows(op, dtype, x, y, row0, row1, accumulate, st);
+  const FFParams& ff = *reinterpret_cast<const FFParams*>(op->ff_params.data());
+  const int64_t D = b.D;
+#define EDK_FF_ROWS(VT)                                                                      \
+  switch (op->tps) {                                                                         \
+    case 2: return launch_apply_ff<VT, 2>(b, op->dev, ff, x, y, 1, D, D, accumulate, st,     \
+                                          row0, row1);                                       \
+    case 4: return launch_apply_ff<VT, 4>(b, op->dev, ff, x, y, 1, D, D, accumulate, st,     \
+                                          row0, row1);                                       \
+    default: return launch_apply_ff<VT, 1>(b, op->dev, ff, x, y, 1, D, D, accumulate, st,    \
+                                           row0, row1);                                      \
+  }
+  switch (dtype) {
+    case EDK_F64: EDK_FF_ROWS(double)
+    case EDK_C128: EDK_FF_ROWS(double2)
+    case EDK_F32: EDK_FF_ROWS(float)
+    case EDK_C64: EDK_FF_ROWS(float2)
+  }
+#undef EDK_FF_ROWS
+  set_error("apply: unknown dtype");
+  return EDK_INVALID_ARG;
+}
+
+}  // namespace edk
 
 extern "C" edk_status edk_operator_create(edk_basis* b, int32_t nterms, const int32_t* nsites,
                                           const int32_t* sites, const int64_t* nnz,
@@ -560,6 +603,30 @@ extern "C" edk_status edk_apply(edk_operator* op, int32_t dtype, const void* x, 
   EDK_TRY_CUDA(cudaMemcpy2DAsync(dx.p, D * es, x, ldx * es, D * es, nvec, cudaMemcpyHostToDevice, st));
   if (accumulate)
     EDK_TRY_CUDA(cudaMemcpy2DAsync(dy.p, D * es, y, ldy * es, D * es, nvec, cudaMemcpyHostToDevice, st));
+  constexpr int64_t kChunkRows = 262144;  // a multiple of every tile height
+  if (nvec == 1 && D >= 2 * kChunkRows && rows_apply_ok(op)) {
+    // pipelined: row chunks computed in order on the operator's stream, each
+    // chunk of y copied back on the copy stream while the next one computes
+    // (psi gathers reach any row, so the input copy cannot be split this way)
+    const int nch = (int)((D + kChunkRows - 1) / kChunkRows);
+    if (!op->cstream) EDK_TRY_CUDA(cudaStreamCreateWithFlags(&op->cstream, cudaStreamNonBlocking));
+    while ((int)op->cevents.size() < nch) {
+      cudaEvent_t e;
+      EDK_TRY_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      op->cevents.push_back(e);
+    }
+    for (int c = 0; c < nch; ++c) {
+      const int64_t r0 = (int64_t)c * kChunkRows, r1 = std::min<int64_t>(D, r0 + kChunkRows);
+      EDK_RETURN_IF(apply_rows(op, dtype, dx.p, dy.p, r0, r1, accumulate, st));
+      EDK_TRY_CUDA(cudaEventRecord(op->cevents[c], st));
+      EDK_TRY_CUDA(cudaStreamWaitEvent(op->cstream, op->cevents[c], 0));
+      EDK_TRY_CUDA(cudaMemcpyAsync((char*)y + r0 * es, (char*)dy.p + r0 * es, (r1 - r0) * es,
+                                   cudaMemcpyDeviceToHost, op->cstream));
+    }
+    EDK_TRY_CUDA(cudaStreamSynchronize(op->cstream));
+    EDK_TRY_CUDA(cudaStreamSynchronize(st));
+    return EDK_OK;
+  }
   EDK_RETURN_IF(apply_device(op, dtype, dx.p, dy.p, nvec, D, D, accumulate, st));
   EDK_TRY_CUDA(cudaMemcpy2DAsync(y, ldy * es, dy.p, D * es, D * es, nvec, cudaMemcpyDeviceToHost, st));
   EDK_TRY_CUDA(cudaStreamSynchronize(st));

@@ -288,6 +288,8 @@ struct edk_operator {
   std::vector<std::vector<int>> sites;
   std::vector<std::vector<double>> dense_re, dense_im;  // local matrices, row-major
   cudaStream_t stream = nullptr;
+  cudaStream_t cstream = nullptr;        // copy stream of the pipelined host path
+  std::vector<cudaEvent_t> cevents;      // one per row chunk of that path
   std::mutex mu;
   ~edk_operator();
 };
@@ -297,7 +299,15 @@ namespace edk {
 edk_status check_basis_dev(const BasisDev& b);
 edk_status index_device(const BasisDev& dv, int64_t n, const uint64_t* s_d, int64_t* p_d,
                         double2* c_d, cudaStream_t st);
+// rows [row0, row1) of y = H x (row0, row1 multiples of 256 or row1 = D)
+// for one vector, on the row-gather fast or materialised paths; false when the
+// operator runs on another path
+bool rows_apply_ok(const edk_operator* op);
+edk_status apply_rows(edk_operator* op, int dtype, const void* x, void* y, int64_t row0,
+                      int64_t row1, int accumulate, cudaStream_t st);
 // implemented in edk_sell.cu
+edk_status apply_sell_rows(edk_operator* op, int dtype, const void* x, void* y, int64_t row0,
+                           int64_t row1, int accumulate, cudaStream_t st);
 edk_status apply_sell(edk_operator* op, int dtype, const void* x, void* y, int64_t nvec,
                       int64_t ldx, int64_t ldy, int accumulate, cudaStream_t st);
 // implemented in edk_apply.cu

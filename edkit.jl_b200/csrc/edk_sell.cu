@@ -184,8 +184,9 @@ __global__ void __launch_bounds__(256) k_sell_fill(BasisDev b, FFParams ff, int6
 template <class VT, int PACKED>
 __global__ void __launch_bounds__(256) k_sell_apply(BasisDev b, SellDev sd,
                                                     const VT* __restrict__ x, VT* __restrict__ y,
-                                                    int64_t ldx, int64_t ldy, int accumulate) {
-  const int64_t slice = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+                                                    int64_t ldx, int64_t ldy, int accumulate,
+                                                    int64_t blk0) {
+  const int64_t slice = (blk0 + blockIdx.x) * 8 + (threadIdx.x >> 5);
   if (slice >= sd.nslices) return;
   sell_slice<VT, PACKED>(b, sd, slice, threadIdx.x & 31, x + (int64_t)blockIdx.y * ldx,
                          y + (int64_t)blockIdx.y * ldy, accumulate);
@@ -208,12 +209,44 @@ static edk_status launch_sell(const BasisDev& b, const SellDev& sd, const void* 
     const VT* xs = static_cast<const VT*>(x) + k0 * ldx;
     VT* ys = static_cast<VT*>(y) + k0 * ldy;
     if (sd.packed)
-      k_sell_apply<VT, 1><<<grid, 256, 0, st>>>(b, sd, xs, ys, ldx, ldy, accumulate);
+      k_sell_apply<VT, 1><<<grid, 256, 0, st>>>(b, sd, xs, ys, ldx, ldy, accumulate, 0);
     else
-      k_sell_apply<VT, 0><<<grid, 256, 0, st>>>(b, sd, xs, ys, ldx, ldy, accumulate);
+      k_sell_apply<VT, 0><<<grid, 256, 0, st>>>(b, sd, xs, ys, ldx, ldy, accumulate, 0);
     EDK_TRY_CUDA(cudaGetLastError());
   }
   return EDK_OK;
+}
+
+// one block = one 256-row window (8 slices), so rows [row0, row1) with
+// row0 a multiple of 256 are windows row0/256 ..
+template <class VT>
+static edk_status launch_sell_rows(const BasisDev& b, const SellDev& sd, const void* x, void* y,
+                                   int64_t row0, int64_t row1, int accumulate, cudaStream_t st) {
+  const int64_t w0 = row0 / 256, w1 = (row1 + 255) / 256;
+  if (w1 <= w0) return EDK_OK;
+  const VT* xs = static_cast<const VT*>(x);
+  VT* ys = static_cast<VT*>(y);
+  const int64_t D = b.D;
+  if (sd.packed)
+    k_sell_apply<VT, 1><<<(unsigned)(w1 - w0), 256, 0, st>>>(b, sd, xs, ys, D, D, accumulate, w0);
+  else
+    k_sell_apply<VT, 0><<<(unsigned)(w1 - w0), 256, 0, st>>>(b, sd, xs, ys, D, D, accumulate, w0);
+  EDK_TRY_CUDA(cudaGetLastError());
+  return EDK_OK;
+}
+
+edk_status apply_sell_rows(edk_operator* op, int dtype, const void* x, void* y, int64_t row0,
+                           int64_t row1, int accumulate, cudaStream_t st) {
+  const BasisDev& b = op->b->dev;
+  const SellDev& sd = op->dev.sell;
+  switch (dtype) {
+    case EDK_F64: return launch_sell_rows<double>(b, sd, x, y, row0, row1, accumulate, st);
+    case EDK_C128: return launch_sell_rows<double2>(b, sd, x, y, row0, row1, accumulate, st);
+    case EDK_F32: return launch_sell_rows<float>(b, sd, x, y, row0, row1, accumulate, st);
+    case EDK_C64: return launch_sell_rows<float2>(b, sd, x, y, row0, row1, accumulate, st);
+  }
+  set_error("apply: unknown dtype");
+  return EDK_INVALID_ARG;
 }
 
 edk_status apply_sell(edk_operator* op, int dtype, const void* x, void* y, int64_t nvec,
