@@ -221,6 +221,50 @@ def run_gpu(args):
                    np.linalg.norm(ref_m - y.cpu().numpy()) / np.linalg.norm(ref_m))}
         H.clear_sparse_cache_()
 
+    # a block of 64 right-hand sides: one SpMM (each hit located once for all
+    # columns) against 64 single-vector passes, matrix-free and materialised
+    blk = None
+    if not args.skip_materialized:
+        nb = 64
+        X = torch.randn((nb, D), dtype=torch.float64, generator=g).to(dev)
+        Y = torch.empty_like(X)
+
+        def blockmv():
+            E.check(lib.edk_apply_async(H._h, E.F64, X.data_ptr(), Y.data_ptr(), nb, D, D, 0,
+                                        stream.cuda_stream))
+
+        def timed(reps=5):
+            for _ in range(2):
+                flush.fill_(1.0)
+                blockmv()
+            torch.cuda.synchronize()
+            evb = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(reps)]
+            for i in range(reps):
+                flush.fill_(float(i))
+                evb[i][0].record(stream)
+                blockmv()
+                evb[i][1].record(stream)
+            torch.cuda.synchronize()
+            return float(np.median([a.elapsed_time(c) for a, c in evb]))
+
+        blk = {"nvec": nb}
+        bb = D * (8 + 8 + nb * 8) + nnz * nb * 8
+        for name, mat_on in (("matrix_free", False), ("materialized", True)):
+            if mat_on:
+                H.sparse_()
+            H.configure_("fast", 1, block=False)
+            t_cols = timed()
+            Yc = Y.clone()
+            H.configure_("fast", 1, block=True)
+            t_blk = timed()
+            blk[name] = {"ms_spmm": round(t_blk, 4), "ms_one_column_at_a_time": round(t_cols, 4),
+                         "speedup": round(t_cols / t_blk, 2),
+                         "GB_s_algorithmic_spmm": round(bb / t_blk / 1e6, 1),
+                         "rel_diff": float((torch.linalg.norm(Y - Yc) / torch.linalg.norm(Yc)).item())}
+        H.clear_sparse_cache_()
+        del X, Y, Yc
+
     # end to end through the C ABI with pinned host buffers
     xh = torch.randn(D, dtype=torch.float64, generator=g).pin_memory()
     yh = torch.empty(D, dtype=torch.float64).pin_memory()
@@ -268,6 +312,8 @@ def run_gpu(args):
         }
         if mat is not None:
             result["matvec_materialized"] = mat
+        if blk is not None:
+            result["block_rhs_64"] = blk
         if not args.skip_e0:
             result["time_to_e0"] = time_to_e0(ek, H, D)
         if args.extras:

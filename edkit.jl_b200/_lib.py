@@ -107,10 +107,10 @@ TUNE_MATERIALIZE = 1
 
 class TuneResult(C.Structure):
     _fields_ = [
-        ("kernel", C.c_int32), ("search", C.c_int32), ("tps", C.c_int32), ("ms", C.c_double),
-        ("ncand", C.c_int32), ("cand_kernel", C.c_int32 * TUNE_MAX),
+        ("kernel", C.c_int32), ("search", C.c_int32), ("tps", C.c_int32), ("block", C.c_int32),
+        ("ms", C.c_double), ("ncand", C.c_int32), ("cand_kernel", C.c_int32 * TUNE_MAX),
         ("cand_search", C.c_int32 * TUNE_MAX), ("cand_tps", C.c_int32 * TUNE_MAX),
-        ("cand_ms", C.c_double * TUNE_MAX),
+        ("cand_block", C.c_int32 * TUNE_MAX), ("cand_ms", C.c_double * TUNE_MAX),
     ]
 
 
@@ -137,7 +137,7 @@ def load():
         "edk_operator_create": (st, [vp, i32, vp, vp, vp, vp, vp, vp, C.POINTER(vp)]),
         "edk_operator_destroy": (st, [vp]),
         "edk_operator_materialize": (st, [vp, i32, C.POINTER(i64)]),
-        "edk_operator_configure": (st, [vp, i32, i32]),
+        "edk_operator_configure": (st, [vp, i32, i32, i32]),
         "edk_operator_autotune": (st, [vp, i32, i64, i32, C.POINTER(TuneResult)]),
         "edk_basis_set_search": (st, [vp, i32]),
         "edk_block_lanczos_default_opts": (None, [C.POINTER(BlockLanczosOpts)]),

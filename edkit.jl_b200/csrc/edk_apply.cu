@@ -25,7 +25,7 @@
 #include <map>
 #include <memory>
 
-#include "edk_rows.cuh"
+#include "edk_spmm.cuh"
 
 namespace edk {
 
@@ -149,6 +149,115 @@ size_t dtype_size(int dtype) {
 
 }  // namespace
 
+namespace {
+
+// column-major (ld) <-> row-major (p) blocks through 32 x 32 shared-memory
+// tiles, coalesced on both sides; the reverse direction can accumulate
+template <class VT>
+__global__ void k_cols_to_rows_t(const VT* __restrict__ src, int64_t ld, int64_t D, int p,
+                                 VT* __restrict__ dst) {
+  __shared__ VT tile[32][33];
+  const int64_t i0 = (int64_t)blockIdx.x * 32;
+  const int c0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int64_t i = i0 + threadIdx.x;
+    const int c = c0 + k;
+    if (i < D && c < p) tile[k][threadIdx.x] = src[(int64_t)c * ld + i];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int64_t i = i0 + k;
+    const int c = c0 + threadIdx.x;
+    if (i < D && c < p) dst[i * p + c] = tile[threadIdx.x][k];
+  }
+}
+
+template <class VT>
+__global__ void k_rows_to_cols_t(const VT* __restrict__ src, int64_t D, int p,
+                                 VT* __restrict__ dst, int64_t ld, int accumulate) {
+  using A = typename VTraits<VT>::A;
+  __shared__ VT tile[32][33];
+  const int64_t i0 = (int64_t)blockIdx.x * 32;
+  const int c0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int64_t i = i0 + k;
+    const int c = c0 + threadIdx.x;
+    if (i < D && c < p) tile[k][threadIdx.x] = src[i * p + c];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int64_t i = i0 + threadIdx.x;
+    const int c = c0 + k;
+    if (i < D && c < p) {
+      VT* d = dst + (int64_t)c * ld + i;
+      if (accumulate) {
+        const Cx<A> a = ldout(d), v = ldout(&tile[threadIdx.x][k]);
+        stv(d, Cx<A>{a.r + v.r, a.i + v.i});
+      } else {
+        *d = tile[threadIdx.x][k];
+      }
+    }
+  }
+}
+
+template <class VT>
+edk_status apply_block_t(edk_operator* op, const void* x, void* y, int64_t nvec, int64_t ldx,
+                         int64_t ldy, int accumulate, cudaStream_t st, int bk, int64_t slots) {
+  const int64_t D = op->b->D;
+  const int pmax = 64;
+  const int pc0 = (int)std::min<int64_t>(nvec, pmax);
+  const size_t need = (size_t)D * pc0 * sizeof(VT);
+  if (op->bx.bytes < need) EDK_RETURN_IF(op->bx.alloc(need));
+  if (op->by.bytes < need) EDK_RETURN_IF(op->by.alloc(need));
+  VT* bx = op->bx.as<VT>();
+  VT* by = op->by.as<VT>();
+  const VT* X = static_cast<const VT*>(x);
+  VT* Y = static_cast<VT*>(y);
+  for (int64_t k0 = 0; k0 < nvec; k0 += pmax) {
+    const int pc = (int)std::min<int64_t>(nvec - k0, pmax);
+    const dim3 tb(32, 8), tg((unsigned)((D + 31) / 32), (unsigned)((pc + 31) / 32));
+    k_cols_to_rows_t<VT><<<tg, tb, 0, st>>>(X + k0 * ldx, ldx, D, pc, bx);
+    EDK_TRY_CUDA(cudaGetLastError());
+    EDK_RETURN_IF(launch_spmm<VT>(op->bop.as<SpmmOp>(), 1, bk, slots, D, pc, bx, by, 0, st));
+    k_rows_to_cols_t<VT><<<tg, tb, 0, st>>>(by, D, pc, Y + k0 * ldy, ldy, accumulate);
+    EDK_TRY_CUDA(cudaGetLastError());
+  }
+  return EDK_OK;
+}
+
+// Several right-hand sides on the row-gather paths: one SpMM over row-major
+// copies of at most 64 columns at a time, so every hit is located once for
+// all of them (false: not applicable, the caller uses the column kernels).
+bool block_apply_ok(const edk_operator* op, int64_t nvec) {
+  return nvec >= 4 && op->gather && (op->sell_ok || (op->ff_ok && op->use_ff && op->b->dev.L <= 32));
+}
+
+edk_status apply_block(edk_operator* op, int dtype, const void* x, void* y, int64_t nvec,
+                       int64_t ldx, int64_t ldy, int accumulate, cudaStream_t st) {
+  SpmmOp h;
+  int bk;
+  int64_t slots;
+  spmm_describe(op, h, bk, slots);
+  std::vector<unsigned char> bytes(sizeof(SpmmOp));
+  std::memcpy(bytes.data(), &h, sizeof(SpmmOp));
+  if (op->bop_host != bytes || !op->bop.p) {
+    if (!op->bop.p) EDK_RETURN_IF(op->bop.alloc(sizeof(SpmmOp)));
+    op->bop_host = bytes;
+    EDK_TRY_CUDA(cudaMemcpyAsync(op->bop.p, op->bop_host.data(), sizeof(SpmmOp),
+                                 cudaMemcpyHostToDevice, st));
+  }
+  switch (dtype) {
+    case EDK_F64: return apply_block_t<double>(op, x, y, nvec, ldx, ldy, accumulate, st, bk, slots);
+    case EDK_C128: return apply_block_t<double2>(op, x, y, nvec, ldx, ldy, accumulate, st, bk, slots);
+    case EDK_F32: return apply_block_t<float>(op, x, y, nvec, ldx, ldy, accumulate, st, bk, slots);
+    case EDK_C64: return apply_block_t<float2>(op, x, y, nvec, ldx, ldy, accumulate, st, bk, slots);
+  }
+  set_error("apply: unknown dtype");
+  return EDK_INVALID_ARG;
+}
+
+}  // namespace
+
 edk_status apply_device(edk_operator* op, int dtype, const void* x, void* y, int64_t nvec,
                         int64_t ldx, int64_t ldy, int accumulate, cudaStream_t st) {
   const BasisDev& b = op->b->dev;
@@ -160,6 +269,8 @@ edk_status apply_device(edk_operator* op, int dtype, const void* x, void* y, int
     EDK_TRY_CUDA(cudaMemset2DAsync(y, ldy * es, 0, b.D * es, nvec, st));
   }
   bool sc = !op->gather;
+  if (block_apply_ok(op, nvec) && (op->use_block > 0 || (op->use_block < 0 && !op->sell_ok)))
+    return apply_block(op, dtype, x, y, nvec, ldx, ldy, accumulate, st);
   if (op->sell_ok && !sc) return apply_sell(op, dtype, x, y, nvec, ldx, ldy, accumulate, st);
   if (op->ff_ok && !sc && op->use_ff) {
     const FFParams& ff = *reinterpret_cast<const FFParams*>(op->ff_params.data());

@@ -35,7 +35,7 @@
 #include <thread>
 #include <vector>
 
-#include "edk_rows.cuh"
+#include "edk_spmm.cuh"
 
 namespace edk {
 
@@ -46,212 +46,6 @@ using cplx = std::complex<double>;
 double wall_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
       .count();
-}
-
-struct BlkOp {
-  BasisDev b;
-  OpDev op;
-  FFParams ff;
-  int64_t D;
-  int kind;  // 0: bond-family SpMM, 1: materialised SpMM, 2: generic (column kernels)
-};
-
-// ---------------------------------------------------------------------------
-// SpMM kernels: Y = H X for every operator, X and Y in the slot layout
-// ---------------------------------------------------------------------------
-template <int BK, int VPL>
-__global__ void __launch_bounds__(256) k_blk_ff(const BlkOp* __restrict__ ops, int nops,
-                                                int64_t Dpad, int p,
-                                                const double2* __restrict__ X,
-                                                double2* __restrict__ Y) {
-  __shared__ uint32_t s_binom[(BK == BK_PROJ_RANK) ? 32 * 33 : 1];
-  if constexpr (BK == BK_PROJ_RANK) {
-    fill_binom32(s_binom);
-    __syncthreads();
-  }
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t total = (int64_t)nops * Dpad;
-  for (int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < total; g += nw) {
-    const int q = (int)(g / Dpad);
-    const int64_t i = g - (int64_t)q * Dpad;
-    const BlkOp& o = ops[q];
-    if (o.kind != 0 || i >= o.D) continue;  // warp-uniform
-    const BasisDev& b = o.b;
-    const FFParams& ff = o.ff;
-    const uint32_t mask = (uint32_t)b.maskL;
-    const uint32_t st = (BK == BK_TENSOR) ? (uint32_t)i : (uint32_t)__ldg(b.I + i);
-    const double invRi = b.R ? 1.0 / __ldg(b.R + i) : 1.0;
-    uint32_t hm[kMaxFF];
-    int cnt[kMaxFF];
-    int nhit = 0;
-    double dr = 0.0, di = 0.0;
-    for (int f = 0; f < ff.nfam; ++f) {
-      const uint32_t Xb = st, Yb = rotl_L(st, ff.d[f], b.L, mask), V = ff.valid[f];
-      const uint32_t m1 = ~Xb & Yb & V, m2 = Xb & ~Yb & V;
-      const int c0 = __popc(~Xb & ~Yb & V), c1 = __popc(m1), c2 = __popc(m2),
-                c3 = __popc(Xb & Yb & V);
-      dr += ff.dval[f][0].x * c0 + ff.dval[f][1].x * c1 + ff.dval[f][2].x * c2 +
-            ff.dval[f][3].x * c3;
-      di += ff.dval[f][0].y * c0 + ff.dval[f][1].y * c1 + ff.dval[f][2].y * c2 +
-            ff.dval[f][3].y * c3;
-      hm[f] = m1 | m2;
-      cnt[f] = __popc(hm[f]);
-      nhit += cnt[f];
-    }
-    for (int t = 0; t < o.op.nterm; ++t) {  // diagonal-only terms
-      const TermDev* T = o.op.term + t;
-      int c = 0;
-      for (int k = 0; k < T->nsites; ++k) c = (c << 1) | (int)((st >> T->bitpos[k]) & 1u);
-      const double2 dv = __ldg(o.op.dval + T->diag_off + c);
-      dr += dv.x;
-      di += dv.y;
-    }
-    const double2* xb = X + (int64_t)q * Dpad * p;
-    double ar[VPL], ai[VPL];
-#pragma unroll
-    for (int v = 0; v < VPL; ++v) {
-      const int c = lane + 32 * v;
-      ar[v] = ai[v] = 0.0;
-      if (c < p) {
-        const double2 xv = __ldg(xb + i * p + c);
-        ar[v] = dr * xv.x + di * xv.y;  // conj(diag) * x
-        ai[v] = dr * xv.y - di * xv.x;
-      }
-    }
-    for (int base = 0; base < nhit; base += 32) {
-      const int l = base + lane;
-      int ok = 0;
-      int64_t pos = 0;
-      double cr = 0.0, ci = 0.0;
-      if (l < nhit) {
-        int f = 0, r = l;
-        while (r >= cnt[f]) { r -= cnt[f]; ++f; }
-        uint32_t m = hm[f];
-        for (int k = 0; k < r; ++k) m &= m - 1;
-        const int pb = __ffs(m) - 1;
-        const int d = ff.d[f];
-        const int qb = pb >= d ? pb - d : pb - d + b.L;
-        HitCtx h;
-        canon_ctx<BK>(b, st ^ (1u << pb) ^ (1u << qb), h);
-        int64_t p1, p2;
-        double r1, r2;
-        bool ok1, ok2;
-        locate2<BK>(b, s_binom, h.key, h.key, false, p1, r1, ok1, p2, r2, ok2);
-        if (ok1) {
-          const double2 w = ((st >> pb) & 1u) ? ff.v2[f] : ff.v1[f];
-          const double ratio = r1 * invRi;
-          cr = (w.x * h.pre - w.y * h.pim) * ratio;
-          ci = (w.x * h.pim + w.y * h.pre) * ratio;
-          pos = p1;
-          ok = 1;
-        }
-      }
-      const int nh = min(32, nhit - base);
-      for (int hh = 0; hh < nh; ++hh) {
-        if (!__shfl_sync(full, ok, hh)) continue;
-        const int64_t ph = __shfl_sync(full, pos, hh);
-        const double crh = __shfl_sync(full, cr, hh), cih = __shfl_sync(full, ci, hh);
-        const double2* xr = xb + ph * p;
-#pragma unroll
-        for (int v = 0; v < VPL; ++v) {
-          const int c = lane + 32 * v;
-          if (c < p) {
-            const double2 xv = __ldg(xr + c);
-            ar[v] += crh * xv.x + cih * xv.y;  // conj(coefficient) * x
-            ai[v] += crh * xv.y - cih * xv.x;
-          }
-        }
-      }
-    }
-    double2* yb = Y + (int64_t)q * Dpad * p + i * p;
-#pragma unroll
-    for (int v = 0; v < VPL; ++v) {
-      const int c = lane + 32 * v;
-      if (c < p) yb[c] = make_double2(ar[v], ai[v]);
-    }
-  }
-}
-
-// materialised operators: one warp per sliced-ELL slot (= one row)
-template <int VPL>
-__global__ void __launch_bounds__(256) k_blk_sell(const BlkOp* __restrict__ ops, int nops,
-                                                  int64_t smax, int64_t Dpad, int p,
-                                                  const double2* __restrict__ X,
-                                                  double2* __restrict__ Y) {
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t total = (int64_t)nops * smax;
-  for (int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < total; g += nw) {
-    const int q = (int)(g / smax);
-    const int64_t s = g - (int64_t)q * smax;
-    const BlkOp& o = ops[q];
-    const SellDev& sd = o.op.sell;
-    if (o.kind != 1 || s >= sd.nslices * 32) continue;
-    const unsigned rc = __ldg(sd.rowid + s);
-    if (rc == ~0u) continue;
-    const int64_t row = rc & ((1u << sd.rbits) - 1u);
-    const double invR = __ldg(sd.rinv + (rc >> sd.rbits));
-    const int64_t slice = s >> 5;
-    const int w = __ldg(sd.width + slice);
-    const int64_t base = __ldg(sd.off + slice) + (s & 31);
-    const double2 d = sd.diagc ? __ldg(sd.diagc + s) : make_double2(__ldg(sd.diag + s), 0.0);
-    const double2* xb = X + (int64_t)q * Dpad * p;
-    double ar[VPL], ai[VPL];
-#pragma unroll
-    for (int v = 0; v < VPL; ++v) {
-      const int c = lane + 32 * v;
-      ar[v] = ai[v] = 0.0;
-      if (c < p) {
-        const double2 xv = __ldg(xb + row * p + c);
-        ar[v] = d.x * xv.x + d.y * xv.y;
-        ai[v] = d.x * xv.y - d.y * xv.x;
-      }
-    }
-    for (int kb = 0; kb < w; kb += 32) {
-      const int k = kb + lane;
-      int col = 0;
-      double cr = 0.0, ci = 0.0;
-      if (k < w) {
-        int code;
-        if (sd.packed) {
-          const unsigned e = __ldg(reinterpret_cast<const unsigned*>(sd.col) + base + (int64_t)k * 32);
-          col = (int)(e >> sd.packed);
-          code = (int)(e & ((1u << sd.packed) - 1u));
-        } else {
-          col = __ldg(sd.col + base + (int64_t)k * 32);
-          code = __ldg(sd.code + base + (int64_t)k * 32);
-        }
-        const double2 v = __ldg(sd.vt64 + code);
-        cr = v.x * invR;
-        ci = v.y * invR;
-      }
-      const int nh = min(32, w - kb);
-      for (int hh = 0; hh < nh; ++hh) {
-        const int ch = __shfl_sync(full, col, hh);
-        const double crh = __shfl_sync(full, cr, hh), cih = __shfl_sync(full, ci, hh);
-        if (crh == 0.0 && cih == 0.0) continue;  // padding entry (code 0)
-        const double2* xr = xb + (int64_t)ch * p;
-#pragma unroll
-        for (int v = 0; v < VPL; ++v) {
-          const int c = lane + 32 * v;
-          if (c < p) {
-            const double2 xv = __ldg(xr + c);
-            ar[v] += crh * xv.x + cih * xv.y;
-            ai[v] += crh * xv.y - cih * xv.x;
-          }
-        }
-      }
-    }
-    double2* yb = Y + (int64_t)q * Dpad * p + row * p;
-#pragma unroll
-    for (int v = 0; v < VPL; ++v) {
-      const int c = lane + 32 * v;
-      if (c < p) yb[c] = make_double2(ar[v], ai[v]);
-    }
-  }
 }
 
 // row-major D x p <-> column-major D x p (ld = D), for operators on the
@@ -306,7 +100,7 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 
 // seeded start blocks: real and imaginary parts N(0, 1) (Box-Muller on two
 // 53-bit uniforms drawn from the counter (seed, operator, row, vector))
-__global__ void k_seed_blocks(const BlkOp* __restrict__ ops, int nops, int64_t Dpad, int p,
+__global__ void k_seed_blocks(const SpmmOp* __restrict__ ops, int nops, int64_t Dpad, int p,
                               uint64_t seed, double2* __restrict__ X) {
   const int64_t total = (int64_t)nops * Dpad * p;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
@@ -704,42 +498,28 @@ static edk_status block_lanczos(int nops, edk_operator* const* ops,
   const size_t slot = (size_t)nops * Dpad * p;
 
   // operator table
-  std::vector<BlkOp> hops(nops);
+  std::vector<SpmmOp> hops(nops);
   bool any_generic = false;
   int64_t smax = 0;
   int bk_ff = -1;
   for (int q = 0; q < nops; ++q) {
-    edk_operator* op = ops[q];
-    EDK_RETURN_IF(check_basis_dev(op->b->dev));
-    BlkOp& h = hops[q];
-    std::memset(&h, 0, sizeof(BlkOp));
-    h.b = op->b->dev;
-    h.op = op->dev;
-    h.D = op->b->D;
-    if (op->sell_ok) {
-      h.kind = 1;
-      smax = std::max<int64_t>(smax, op->dev.sell.nslices * 32);
-    } else if (op->ff_ok && op->use_ff && op->b->dev.L <= 32) {
-      h.kind = 0;
-      std::memcpy(&h.ff, op->ff_params.data(), sizeof(FFParams));
-      int bk = op->b->dev.bk;
-      if (bk == BK_TRANS0) bk = BK_TRANS;  // one instantiation covers both
+    EDK_RETURN_IF(check_basis_dev(ops[q]->b->dev));
+    int bk;
+    int64_t slots;
+    const int kind = spmm_describe(ops[q], hops[q], bk, slots);
+    if (kind == 1) smax = std::max<int64_t>(smax, slots);
+    if (kind == 2) any_generic = true;
+    if (kind == 0) {
       if (bk_ff >= 0 && bk_ff != bk) {
         set_error("edk_block_lanczos: operators on different kinds of basis in one batch");
         return EDK_UNSUPPORTED;
       }
       bk_ff = bk;
-    } else {
-      h.kind = 2;
-      any_generic = true;
     }
   }
-  if (bk_ff == BK_TRANS)
-    for (auto& h : hops)
-      if (h.kind == 0 && h.b.bk == BK_TRANS0) h.b.bk = BK_TRANS;
 
   DevBuf d_ops, ring0, ring1, ring2, part, Q1, Q2, Q1b, Q2b, G, Rinv, R1, R2, Bm, flags, colx, coly;
-  EDK_RETURN_IF(d_ops.alloc(sizeof(BlkOp) * nops));
+  EDK_RETURN_IF(d_ops.alloc(sizeof(SpmmOp) * nops));
   EDK_RETURN_IF(ring0.alloc(slot * sizeof(double2)));
   EDK_RETURN_IF(ring1.alloc(slot * sizeof(double2)));
   EDK_RETURN_IF(ring2.alloc(slot * sizeof(double2)));
@@ -751,7 +531,7 @@ static edk_status block_lanczos(int nops, edk_operator* const* ops,
     EDK_RETURN_IF(colx.alloc((size_t)Dmax * p * sizeof(double2)));
     EDK_RETURN_IF(coly.alloc((size_t)Dmax * p * sizeof(double2)));
   }
-  EDK_TRY_CUDA(cudaMemcpyAsync(d_ops.p, hops.data(), sizeof(BlkOp) * nops,
+  EDK_TRY_CUDA(cudaMemcpyAsync(d_ops.p, hops.data(), sizeof(SpmmOp) * nops,
                                cudaMemcpyHostToDevice, st));
   EDK_TRY_CUDA(cudaMemsetAsync(flags.p, 0, nops * sizeof(int), st));
   for (DevBuf* bf : {&ring0, &ring1, &ring2})
@@ -831,37 +611,8 @@ static edk_status block_lanczos(int nops, edk_operator* const* ops,
   } evg{e0, e1, e2};
 
   auto spmm = [&](const double2* X, double2* Y) -> edk_status {
-    const int VPL = p > 32 ? 2 : 1;
-    if (bk_ff >= 0) {
-      const int64_t nw = (int64_t)nops * Dpad;
-      const int grid = (int)std::min<int64_t>((nw + 7) / 8, 148 * 64);
-#define EDK_BLK_FF(BK)                                                                            \
-  case BK:                                                                                        \
-    if (VPL == 2) k_blk_ff<BK, 2><<<grid, 256, 0, st>>>(d_ops.as<BlkOp>(), nops, Dpad, p, X, Y); \
-    else k_blk_ff<BK, 1><<<grid, 256, 0, st>>>(d_ops.as<BlkOp>(), nops, Dpad, p, X, Y);          \
-    break;
-      switch (bk_ff) {
-        EDK_BLK_FF(BK_TENSOR)
-        EDK_BLK_FF(BK_PROJ_RANK)
-        EDK_BLK_FF(BK_PROJ_HASH)
-        EDK_BLK_FF(BK_TRANS)
-        EDK_BLK_FF(BK_TRANSPAR)
-        default:
-          set_error("edk_block_lanczos: unsupported basis kind for the bond-family SpMM");
-          return EDK_UNSUPPORTED;
-      }
-#undef EDK_BLK_FF
-      EDK_TRY_CUDA(cudaGetLastError());
-    }
-    if (smax > 0) {
-      const int64_t nw = (int64_t)nops * smax;
-      const int grid = (int)std::min<int64_t>((nw + 7) / 8, 148 * 64);
-      if (VPL == 2)
-        k_blk_sell<2><<<grid, 256, 0, st>>>(d_ops.as<BlkOp>(), nops, smax, Dpad, p, X, Y);
-      else
-        k_blk_sell<1><<<grid, 256, 0, st>>>(d_ops.as<BlkOp>(), nops, smax, Dpad, p, X, Y);
-      EDK_TRY_CUDA(cudaGetLastError());
-    }
+    EDK_RETURN_IF(launch_spmm<double2>(d_ops.as<SpmmOp>(), nops, bk_ff, smax, Dpad, p, X, Y, 0,
+                                       st));
     if (any_generic) {
       for (int q = 0; q < nops; ++q) {
         if (hops[q].kind != 2) continue;
@@ -897,7 +648,7 @@ static edk_status block_lanczos(int nops, edk_operator* const* ops,
       EDK_TRY_CUDA(cudaStreamSynchronize(st));
     }
   } else {
-    k_seed_blocks<<<grid_for((int64_t)nops * Dpad * p), 256, 0, st>>>(d_ops.as<BlkOp>(), nops,
+    k_seed_blocks<<<grid_for((int64_t)nops * Dpad * p), 256, 0, st>>>(d_ops.as<SpmmOp>(), nops,
                                                                       Dpad, p, o.seed, W);
     EDK_TRY_CUDA(cudaGetLastError());
   }

@@ -281,6 +281,8 @@ struct edk_operator {
   bool ff_ok = false;     // flip-flop bond-family fast path applies
   bool use_ff = true;     // callers may switch the fast path off (A/B checks)
   int tps = 1;            // threads per state of the fast path (1, 2 or 4; autotuned)
+  int use_block = -1;     // several right-hand sides through one SpMM: 1 yes, 0 no, -1 auto
+                          // (matrix-free yes, materialised no: its SpMV already streams)
   std::vector<unsigned char> ff_params;
   int max_hits = 0;
   int nfam = 0, ngeneric = 0;
@@ -288,6 +290,8 @@ struct edk_operator {
   std::vector<std::vector<int>> sites;
   std::vector<std::vector<double>> dense_re, dense_im;  // local matrices, row-major
   cudaStream_t stream = nullptr;
+  edk::DevBuf bx, by, bop;               // row-major blocks and operator record of the SpMM path
+  std::vector<unsigned char> bop_host;   // the record as last uploaded
   cudaStream_t cstream = nullptr;        // copy stream of the pipelined host path
   std::vector<cudaEvent_t> cevents;      // one per row chunk of that path
   std::mutex mu;

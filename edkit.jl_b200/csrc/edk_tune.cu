@@ -56,7 +56,8 @@ edk_status time_apply(edk_operator* op, int dtype, const void* x, void* y, int64
 
 }  // namespace
 
-extern "C" edk_status edk_operator_configure(edk_operator* op, int32_t kernel, int32_t tps) {
+extern "C" edk_status edk_operator_configure(edk_operator* op, int32_t kernel, int32_t tps,
+                                             int32_t block) {
   EDK_CHECK_ARG(op != nullptr, "edk_operator_configure: NULL operator");
   EDK_CHECK_ARG(kernel == EDK_KERNEL_FAST || kernel == EDK_KERNEL_GENERIC,
                 "edk_operator_configure: kernel must be EDK_KERNEL_FAST or EDK_KERNEL_GENERIC");
@@ -69,6 +70,7 @@ extern "C" edk_status edk_operator_configure(edk_operator* op, int32_t kernel, i
   }
   op->use_ff = kernel == EDK_KERNEL_FAST;
   op->tps = tps;
+  op->use_block = block < 0 ? -1 : (block != 0);
   return EDK_OK;
 }
 
@@ -102,16 +104,23 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
   std::vector<int> searches{EDK_SEARCH_HASH};
   if (has_search && edk_basis_set_search(b, EDK_SEARCH_SORTED) == EDK_OK)
     searches.push_back(EDK_SEARCH_SORTED);
-  struct Cand { int kernel, search, tps; };
+  struct Cand { int kernel, search, tps, block; };
   std::vector<Cand> cands;
   const bool fast = op->ff_ok && op->gather;
+  // several right-hand sides: the bond-family and materialised kernels also
+  // run as one SpMM over the block (block = 1)
+  const bool multi = nvec >= 4 && op->gather;
   for (int s : searches) {
     if (fast)
-      for (int t : {1, 2, 4}) cands.push_back({EDK_KERNEL_FAST, s, t});
-    cands.push_back({EDK_KERNEL_GENERIC, s, 1});
+      for (int t : {1, 2, 4}) cands.push_back({EDK_KERNEL_FAST, s, t, 0});
+    if (fast && multi && op->b->dev.L <= 32) cands.push_back({EDK_KERNEL_FAST, s, 1, 1});
+    cands.push_back({EDK_KERNEL_GENERIC, s, 1, 0});
   }
   const bool was_mat = op->sell_ok;
-  if ((flags & EDK_TUNE_MATERIALIZE) || was_mat) cands.push_back({EDK_KERNEL_MATERIALIZED, 0, 1});
+  if ((flags & EDK_TUNE_MATERIALIZE) || was_mat) {
+    cands.push_back({EDK_KERNEL_MATERIALIZED, 0, 1, 0});
+    if (multi) cands.push_back({EDK_KERNEL_MATERIALIZED, 0, 1, 1});
+  }
 
   const int reps = 7;
   double best = 1e300, best_free = 1e300;
@@ -127,6 +136,7 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
       op->use_ff = c.kernel == EDK_KERNEL_FAST;
       op->tps = c.tps;
     }
+    op->use_block = c.block;
     {
       std::lock_guard<std::mutex> lk(op->mu);
       rc = time_apply(op, dtype, x.p, y.p, nvec, reps, ms);
@@ -136,6 +146,7 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
       out.cand_kernel[out.ncand] = c.kernel;
       out.cand_search[out.ncand] = c.search;
       out.cand_tps[out.ncand] = c.tps;
+      out.cand_block[out.ncand] = c.block;
       out.cand_ms[out.ncand] = ms;
       ++out.ncand;
     }
@@ -149,10 +160,12 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
   if (has_search) edk_basis_set_search(b, pick_free.search);
   op->use_ff = pick_free.kernel == EDK_KERNEL_FAST;
   op->tps = pick_free.tps;
+  op->use_block = multi ? (pick.kernel == EDK_KERNEL_MATERIALIZED ? pick : pick_free).block : -1;
   if (pick.kernel == EDK_KERNEL_MATERIALIZED) EDK_RETURN_IF(edk_operator_materialize(op, 1, nullptr));
   out.kernel = pick.kernel;
   out.search = b->dev.search ? EDK_SEARCH_SORTED : EDK_SEARCH_HASH;
   out.tps = pick_free.tps;
+  out.block = pick.block;
   out.ms = best;
   if (res) *res = out;
   return EDK_OK;

@@ -215,9 +215,9 @@ clear_sparse!(H::B200Operator) =
                 H.h, 0, C_NULL))
 
 struct TuneResult
-    kernel::Int32; search::Int32; tps::Int32; ms::Float64; ncand::Int32
+    kernel::Int32; search::Int32; tps::Int32; block::Int32; ms::Float64; ncand::Int32
     cand_kernel::NTuple{24, Int32}; cand_search::NTuple{24, Int32}; cand_tps::NTuple{24, Int32}
-    cand_ms::NTuple{24, Float64}
+    cand_block::NTuple{24, Int32}; cand_ms::NTuple{24, Float64}
 end
 
 """

@@ -295,10 +295,13 @@ class Operator:
 
     _KERNELS = {"fast": 0, "generic": 1, "materialized": 2}
 
-    def configure_(self, kernel="fast", tps=1):
+    def configure_(self, kernel="fast", tps=1, block=None):
         """Pick the matrix-free kernel by hand: "fast" (bond families, `tps`
-        threads per state) or "generic"; both give the same product."""
-        E.check(E.load().edk_operator_configure(self._h, self._KERNELS[kernel], int(tps)))
+        threads per state) or "generic"; `block` True/False forces four or
+        more right-hand sides through one SpMM or one column at a time (None:
+        automatic).  Every choice gives the same product."""
+        E.check(E.load().edk_operator_configure(self._h, self._KERNELS[kernel], int(tps),
+                                                -1 if block is None else int(bool(block))))
 
     def autotune_(self, dtype=None, nvec=1, materialize=False):
         """Time every admissible kernel / threads-per-state / index-search
@@ -312,9 +315,11 @@ class Operator:
         names = {v: k for k, v in self._KERNELS.items()}
         srch = {0: "hash", 1: "sorted"}
         self.materialized = r.kernel == E.KERNEL_MATERIALIZED
-        return {"kernel": names[r.kernel], "search": srch[r.search], "tps": r.tps, "ms": r.ms,
+        return {"kernel": names[r.kernel], "search": srch[r.search], "tps": r.tps,
+                "block": bool(r.block), "ms": r.ms,
                 "candidates": [(names[r.cand_kernel[i]], srch[r.cand_search[i]], r.cand_tps[i],
-                                r.cand_ms[i]) for i in range(r.ncand)]}
+                                r.cand_ms[i]) for i in range(r.ncand)],
+                "candidates_block": [bool(r.cand_block[i]) for i in range(r.ncand)]}
 
     def todense(self):
         """Array(opt) — Operator.jl:171-196 (H times the identity, small D only)."""

@@ -203,28 +203,34 @@ edk_status edk_block_lanczos(int32_t nops, edk_operator* const* ops,
 /* Kernel choice of the matrix-free application.  EDK_KERNEL_FAST: the
  * bond-family kernel (operators whose off-diagonal part is flip-flop bonds),
  * with `tps` threads (1, 2, 4) sharing each state; EDK_KERNEL_GENERIC: the
- * row kernel that handles every operator.  Both compute the same product as
- * EDKit's mul! (Operator.jl:309-328).  No reference counterpart as a call:
- * EDKit has one CPU kernel. */
+ * row kernel that handles every operator.  block = 1 applies four or more
+ * right-hand sides as one SpMM on the bond-family and materialised paths
+ * (each nonzero located once for all columns, as colmn! does,
+ * Operator.jl:417-465); block = 0 runs them one column at a time; block = -1
+ * (the default) uses the SpMM matrix-free and the columns on a materialised
+ * matrix.  Every
+ * choice computes the same product as EDKit's mul! (Operator.jl:309-328).
+ * No reference counterpart as a call: EDKit has one CPU kernel. */
 #define EDK_KERNEL_FAST 0
 #define EDK_KERNEL_GENERIC 1
 #define EDK_KERNEL_MATERIALIZED 2
-edk_status edk_operator_configure(edk_operator* op, int32_t kernel, int32_t tps);
+edk_status edk_operator_configure(edk_operator* op, int32_t kernel, int32_t tps, int32_t block);
 
 /* Autotuner: times every admissible (kernel, threads per state, index
  * search) combination — and, with EDK_TUNE_MATERIALIZE or when the operator
  * is already materialised, the materialised matrix — applying the operator to
- * `nvec` vectors of `dtype`, then installs the fastest matrix-free choice
+ * `nvec` vectors of `dtype` (with nvec >= 4 also the SpMM form), then installs the fastest matrix-free choice
  * (index search on the basis, kernel and tps on the operator) and, when it
  * wins, the materialised matrix on top (kept only then).  Allocates two nvec x D work vectors for the duration.  Not
  * to be called while other calls use the operator or its basis. */
 #define EDK_TUNE_MATERIALIZE 1
 #define EDK_TUNE_MAX 24
 typedef struct {
-  int32_t kernel, search, tps;  /* the choice installed */
-  double ms;                    /* its median time per application */
-  int32_t ncand;                /* candidates timed */
-  int32_t cand_kernel[EDK_TUNE_MAX], cand_search[EDK_TUNE_MAX], cand_tps[EDK_TUNE_MAX];
+  int32_t kernel, search, tps, block;  /* the choice installed */
+  double ms;                           /* its median time per application */
+  int32_t ncand;                       /* candidates timed */
+  int32_t cand_kernel[EDK_TUNE_MAX], cand_search[EDK_TUNE_MAX], cand_tps[EDK_TUNE_MAX],
+      cand_block[EDK_TUNE_MAX];
   double cand_ms[EDK_TUNE_MAX];
 } edk_tune_result;
 edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int64_t nvec, int32_t flags,
