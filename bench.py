@@ -317,6 +317,7 @@ def run_gpu(args):
         if not args.skip_e0:
             result["time_to_e0"] = time_to_e0(ek, H, D)
         if args.extras:
+            result["config1_tensor_L16"] = config1_tensor(ek)
             result["config5_random_field_ensemble"] = config5_ensemble(ek)
             result["config4_momentum_sectors"] = config4_sectors(ek)
             result["config3_krylov_L32"] = config3_krylov(ek)
@@ -368,6 +369,45 @@ def time_to_e0(ek, H, D):
         "speedup_mixed_materialized_vs_fp64_matrix_free": round(d64["seconds"] / dmxm["seconds"], 3),
         "dE0_rel_mixed_vs_fp64": abs(emxm[0] - e64[0]) / abs(e64[0])}
     return out
+
+
+def config1_tensor(ek, steps=150):
+    """Open XXZ L=16, Delta=1.5 on the TensorBasis (D=65536), ComplexF64 psi
+    with seeded normal parts, normalised: one H*psi and a 150-step Lanczos for
+    E0 on the GPU; the oracle's threaded mul on the host for the same psi."""
+    import torch
+    import oracle as O
+    L = 16
+    b = ek.TensorBasis(L=L)
+    inds = [[i, i + 1] for i in range(1, L)]
+    bond = ek.spin((1.0, "xx"), (1.0, "yy"), (1.5, "zz"))
+    H = ek.operator([bond] * (L - 1), inds, b)
+    rng = np.random.default_rng(1234)
+    psi = rng.standard_normal(2 ** L) + 1j * rng.standard_normal(2 ** L)
+    psi /= np.linalg.norm(psi)
+    x = torch.from_numpy(psi).cuda()
+    for _ in range(3):
+        y = H * x
+    torch.cuda.synchronize()
+    a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(20):
+        y = H * x
+    c.record()
+    torch.cuda.synchronize()
+    res = {"D": 2 ** L, "matvec_ms": round(a.elapsed_time(c) / 20, 4)}
+    for _ in range(2):
+        ev, d = ek.lanczos_e0(H, psi, m=steps)
+    res["lanczos150"] = {"seconds": round(d["seconds"], 4), "E0": float(ev[0])}
+    o = O.tensor(L)
+    Ho = O.operator([O.spin((1.0, "xx"), (1.0, "yy"), (1.5, "zz"))] * (L - 1), inds, o)
+    Ho.mul(psi)
+    t = time.perf_counter()
+    yo = Ho.mul(psi)
+    res["cpu_oracle_mul_ms"] = round((time.perf_counter() - t) * 1e3, 3)
+    res["cpu_oracle_threads"] = os.cpu_count()
+    res["rel_diff_vs_oracle"] = float(np.linalg.norm(y.cpu().numpy() - yo) / np.linalg.norm(yo))
+    return res
 
 
 def config5_ensemble(ek, n_inst=512, seed=2024, steps=200):

@@ -100,7 +100,7 @@ class BlockLanczosDiag(C.Structure):
 
 
 TUNE_MAX = 24
-KERNEL_FAST, KERNEL_GENERIC, KERNEL_MATERIALIZED = 0, 1, 2
+KERNEL_FAST, KERNEL_GENERIC, KERNEL_MATERIALIZED, KERNEL_MATERIALIZED_STAGED = 0, 1, 2, 3
 SEARCH_HASH, SEARCH_SORTED = 0, 1
 TUNE_MATERIALIZE = 1
 

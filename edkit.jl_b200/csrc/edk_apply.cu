@@ -670,6 +670,19 @@ extern "C" edk_status edk_operator_info(const edk_operator* op, int32_t* gather,
   return EDK_OK;
 }
 
+// after a synchronised product: a bounded wait of the staged materialised
+// kernel that ran out (never expected) is reported instead of a silent result
+static edk_status staged_status(edk_operator* op) {
+  if (!(op->sell_ok && op->sell_tma && op->sell_tma_ok && op->s_err.p)) return EDK_OK;
+  int err = 0;
+  EDK_TRY_CUDA(cudaMemcpy(&err, op->s_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    set_error("apply: the staged materialised product timed out waiting for its copies");
+    return EDK_TIMEOUT;
+  }
+  return EDK_OK;
+}
+
 static edk_status check_dtype(const edk_operator* op, int dtype) {
   EDK_CHECK_ARG(dtype >= EDK_F64 && dtype <= EDK_C64, "apply: unknown dtype");
   if (op->is_complex && (dtype == EDK_F64 || dtype == EDK_F32)) {
@@ -701,7 +714,7 @@ extern "C" edk_status edk_apply(edk_operator* op, int32_t dtype, const void* x, 
   if (ptr_kind == EDK_DEVICE) {
     EDK_RETURN_IF(apply_device(op, dtype, x, y, nvec, ldx, ldy, accumulate, st));
     EDK_TRY_CUDA(cudaStreamSynchronize(st));
-    return EDK_OK;
+    return staged_status(op);
   }
   EDK_CHECK_ARG(ptr_kind == EDK_HOST, "edk_apply: bad ptr_kind");
   if (nvec == 0 || D == 0) return EDK_OK;
@@ -736,10 +749,10 @@ extern "C" edk_status edk_apply(edk_operator* op, int32_t dtype, const void* x, 
     }
     EDK_TRY_CUDA(cudaStreamSynchronize(op->cstream));
     EDK_TRY_CUDA(cudaStreamSynchronize(st));
-    return EDK_OK;
+    return staged_status(op);
   }
   EDK_RETURN_IF(apply_device(op, dtype, dx.p, dy.p, nvec, D, D, accumulate, st));
   EDK_TRY_CUDA(cudaMemcpy2DAsync(y, ldy * es, dy.p, D * es, D * es, nvec, cudaMemcpyDeviceToHost, st));
   EDK_TRY_CUDA(cudaStreamSynchronize(st));
-  return EDK_OK;
+  return staged_status(op);
 }

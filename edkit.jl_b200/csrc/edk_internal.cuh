@@ -272,7 +272,10 @@ struct edk_operator {
   edk::DevBuf fam, term, colptr, xmask, val, dval;
   edk::DevBuf hx, hy;  // staging buffers of edk_apply's host-pointer path (grow only)
   // materialised matrix (edk_operator_materialize)
-  edk::DevBuf s_rowid, s_off, s_width, s_col, s_code, s_diag, s_vt64, s_vt32, s_rinv;
+  edk::DevBuf s_rowid, s_off, s_width, s_col, s_code, s_diag, s_vt64, s_vt32, s_rinv, s_err;
+  int64_t sell_wincap = 0;  // entries of the largest 256-row window
+  bool sell_tma_ok = false;  // the staged (bulk-copy) product applies (stages fit in shared memory)
+  bool sell_tma = false;     // ... and is used (set by the autotuner)
   bool sell_ok = false;
   int64_t sell_entries = 0;
   edk::OpDev dev{};

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "edk_rows.cuh"
+#include "edk_tma.cuh"
 
 namespace edk {
 
@@ -192,12 +193,168 @@ __global__ void __launch_bounds__(256) k_sell_apply(BasisDev b, SellDev sd,
                          y + (int64_t)blockIdx.y * ldy, accumulate);
 }
 
+// Materialised product with the entry stream staged through shared memory:
+// a persistent block walks windows wbeg + blockIdx.x + i * gridDim.x; thread 0
+// copies each window's packed entries (8 slices, contiguous in `col`) with one
+// bulk asynchronous copy into one of two stages, two windows ahead, so the
+// lanes read their entries from shared memory and only the psi gathers stay
+// in the dependent-latency chain.  Waits are bounded: a wait that runs out
+// raises *err and the block stops.
+template <class VT>
+__global__ void __launch_bounds__(256) k_sell_tma(BasisDev b, SellDev sd,
+                                                  const VT* __restrict__ x, VT* __restrict__ y,
+                                                  int accumulate, int64_t wbeg, int64_t wend,
+                                                  int cap_words, int* __restrict__ err) {
+  using A = typename VTraits<VT>::A;
+  constexpr bool CX = VTraits<VT>::cx;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);  // two barriers, then the stages
+  unsigned* const stage0 = reinterpret_cast<unsigned*>(smem_raw + 128);
+  auto stage_buf = [&](int stage) { return stage0 + (stage ? cap_words : 0); };
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  if (t == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto window_end = [&](int64_t w) -> int64_t {  // entry offset past window w
+    const int64_t s1 = min(w * 8 + 8, sd.nslices);
+    return __ldg(sd.off + s1 - 1) + (int64_t)__ldg(sd.width + s1 - 1) * 32;
+  };
+  auto issue = [&](int64_t w, int stage) {  // thread 0
+    const int64_t e0 = __ldg(sd.off + w * 8);
+    const uint32_t bytes = (uint32_t)((window_end(w) - e0) * 4);
+    if (bytes) {
+      mbar_arrive_expect_tx(&bar[stage], bytes);
+      bulk_copy_g2s(stage_buf(stage), reinterpret_cast<const unsigned*>(sd.col) + e0, bytes,
+                    &bar[stage]);
+    } else {
+      mbar_arrive(&bar[stage]);
+    }
+  };
+  const int64_t step = gridDim.x;
+  const int64_t w0 = wbeg + blockIdx.x;
+  if (t == 0) {
+    if (w0 < wend) issue(w0, 0);
+    if (w0 + step < wend) issue(w0 + step, 1);
+  }
+  const int sh = sd.packed;
+  const unsigned cm = (1u << sh) - 1u;
+  int i = 0;
+  for (int64_t w = w0; w < wend; w += step, ++i) {
+    const int stage = i & 1;
+    const bool ok = mbar_wait_bounded(&bar[stage], (uint32_t)((i >> 1) & 1), 1u << 20);
+    if (__syncthreads_or(!ok)) {
+      if (t == 0) atomicExch(err, 1);
+      return;
+    }
+    const int64_t slice = w * 8 + warp;
+    if (slice < sd.nslices) {
+      const int64_t eoff = __ldg(sd.off + slice) - __ldg(sd.off + w * 8);
+      const unsigned* ep = stage_buf(stage) + eoff + lane;
+      const int wd = __ldg(sd.width + slice);
+      const unsigned rc = __ldg(sd.rowid + slice * 32 + lane);
+      A ar = 0, ai = 0;
+      auto term = [&](unsigned e) {
+        const int c = (int)(e >> sh), code = (int)(e & cm);
+        const Cx<A> xv = ldv(x + c);
+        if constexpr (CX) {
+          A vr, vi;
+          if constexpr (sizeof(A) == 8) {
+            const double2 v = __ldg(sd.vt64 + code);
+            vr = v.x; vi = v.y;
+          } else {
+            const float2 v = __ldg(sd.vt32 + code);
+            vr = v.x; vi = v.y;
+          }
+          ar += vr * xv.r + vi * xv.i;  // conj(v) * x
+          ai += vr * xv.i - vi * xv.r;
+        } else {
+          A vr;
+          if constexpr (sizeof(A) == 8)
+            vr = __ldg(reinterpret_cast<const double*>(sd.vt64) + 2 * code);
+          else
+            vr = __ldg(reinterpret_cast<const float*>(sd.vt32) + 2 * code);
+          ar += vr * xv.r;
+        }
+      };
+      int k = 0;
+      for (; k + 4 <= wd; k += 4) {
+        const unsigned e0 = ep[(k + 0) * 32], e1 = ep[(k + 1) * 32];
+        const unsigned e2 = ep[(k + 2) * 32], e3 = ep[(k + 3) * 32];
+        term(e0);
+        term(e1);
+        term(e2);
+        term(e3);
+      }
+      for (; k < wd; ++k) term(ep[k * 32]);
+      if (rc != ~0u) {
+        const int64_t row = rc & ((1u << sd.rbits) - 1u);
+        const A invR = (A)__ldg(sd.rinv + (rc >> sd.rbits));
+        const double2 d =
+            sd.diagc ? __ldg(sd.diagc + slice * 32 + lane) : make_double2(__ldg(sd.diag + slice * 32 + lane), 0.0);
+        const Cx<A> xi = ldv(x + row);
+        Cx<A> out{ar * invR + (A)d.x * xi.r + (A)d.y * xi.i, (A)0};
+        if constexpr (CX) out.i = ai * invR + (A)d.x * xi.i - (A)d.y * xi.r;
+        if (accumulate) {
+          const Cx<A> yo = ldout(y + row);
+          out.r += yo.r;
+          out.i += yo.i;
+        }
+        stv(y + row, out);
+      }
+    }
+    __syncthreads();  // every lane is done with this stage
+    if (t == 0 && w + 2 * step < wend) {
+      fence_proxy_async_smem();
+      issue(w + 2 * step, stage);
+    }
+  }
+}
+
 int gridn(int64_t n) {
   int64_t g = (n + 255) / 256;
   return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
 }
 
 }  // namespace
+
+// the staged kernel for windows [w0, w1); false when it does not apply
+template <class VT>
+static bool launch_sell_tma(edk_operator* op, const void* x, void* y, int accumulate,
+                            int64_t w0, int64_t w1, cudaStream_t st, edk_status& rc) {
+  const SellDev& sd = op->dev.sell;
+  rc = EDK_OK;
+  if (!sd.packed || !op->sell_tma || !op->sell_tma_ok || w1 <= w0) return false;
+  const size_t smem = 128 + 2 * (size_t)op->sell_wincap * 4;
+  static thread_local int attr_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    cudaFuncSetAttribute(k_sell_tma<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(k_sell_tma<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(k_sell_tma<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(k_sell_tma<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    attr_dev = dev;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sell_tma<VT>, 256, smem) !=
+          cudaSuccess || per_sm < 1)
+    return false;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t grid = std::min<int64_t>(w1 - w0, (int64_t)nsm * per_sm);
+  k_sell_tma<VT><<<(unsigned)grid, 256, smem, st>>>(op->b->dev, sd, static_cast<const VT*>(x),
+                                                    static_cast<VT*>(y), accumulate, w0, w1,
+                                                    (int)op->sell_wincap, op->s_err.as<int>());
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(std::string("k_sell_tma launch failed: ") + cudaGetErrorString(e));
+    rc = EDK_CUDA_ERROR;
+  }
+  return true;
+}
 
 template <class VT>
 static edk_status launch_sell(const BasisDev& b, const SellDev& sd, const void* x, void* y,
@@ -239,6 +396,18 @@ edk_status apply_sell_rows(edk_operator* op, int dtype, const void* x, void* y, 
                            int64_t row1, int accumulate, cudaStream_t st) {
   const BasisDev& b = op->b->dev;
   const SellDev& sd = op->dev.sell;
+  {
+    const int64_t w0 = row0 / 256, w1 = (row1 + 255) / 256;
+    edk_status rc = EDK_OK;
+    bool done = false;
+    switch (dtype) {
+      case EDK_F64: done = launch_sell_tma<double>(op, x, y, accumulate, w0, w1, st, rc); break;
+      case EDK_C128: done = launch_sell_tma<double2>(op, x, y, accumulate, w0, w1, st, rc); break;
+      case EDK_F32: done = launch_sell_tma<float>(op, x, y, accumulate, w0, w1, st, rc); break;
+      case EDK_C64: done = launch_sell_tma<float2>(op, x, y, accumulate, w0, w1, st, rc); break;
+    }
+    if (done) return rc;
+  }
   switch (dtype) {
     case EDK_F64: return launch_sell_rows<double>(b, sd, x, y, row0, row1, accumulate, st);
     case EDK_C128: return launch_sell_rows<double2>(b, sd, x, y, row0, row1, accumulate, st);
@@ -253,6 +422,18 @@ edk_status apply_sell(edk_operator* op, int dtype, const void* x, void* y, int64
                       int64_t ldx, int64_t ldy, int accumulate, cudaStream_t st) {
   const BasisDev& b = op->b->dev;
   const SellDev& sd = op->dev.sell;
+  if (nvec == 1) {
+    const int64_t nwin = (sd.nslices + 7) / 8;
+    edk_status rc = EDK_OK;
+    bool done = false;
+    switch (dtype) {
+      case EDK_F64: done = launch_sell_tma<double>(op, x, y, accumulate, 0, nwin, st, rc); break;
+      case EDK_C128: done = launch_sell_tma<double2>(op, x, y, accumulate, 0, nwin, st, rc); break;
+      case EDK_F32: done = launch_sell_tma<float>(op, x, y, accumulate, 0, nwin, st, rc); break;
+      case EDK_C64: done = launch_sell_tma<float2>(op, x, y, accumulate, 0, nwin, st, rc); break;
+    }
+    if (done) return rc;
+  }
   switch (dtype) {
     case EDK_F64: return launch_sell<double>(b, sd, x, y, nvec, ldx, ldy, accumulate, st);
     case EDK_C128: return launch_sell<double2>(b, sd, x, y, nvec, ldx, ldy, accumulate, st);
@@ -424,6 +605,19 @@ static edk_status materialize(edk_operator* op) {
   sd.rinv = op->s_rinv.as<double>();
   sd.vt64 = op->s_vt64.as<double2>();
   sd.vt32 = op->s_vt32.as<float2>();
+  // largest window (8 slices) in entries: the stage size of the staged kernel
+  int64_t wincap = 0;
+  for (int64_t wdx = 0; wdx < nwin; ++wdx) {
+    int64_t ew = 0;
+    for (int sl = 0; sl < 8; ++sl) ew += (int64_t)width[wdx * 8 + sl] * 32;
+    wincap = std::max(wincap, ew);
+  }
+  op->sell_wincap = wincap;
+  op->sell_tma_ok = packed != 0 && 128 + 2 * wincap * 4 <= 200 * 1024;
+  op->sell_tma = false;  // the autotuner enables it where it measures faster
+  EDK_RETURN_IF(op->s_err.alloc(sizeof(int)));
+  EDK_TRY_CUDA(cudaMemsetAsync(op->s_err.p, 0, sizeof(int), st));
+  EDK_TRY_CUDA(cudaStreamSynchronize(st));
   op->sell_entries = E;
   op->sell_ok = true;
   return EDK_OK;

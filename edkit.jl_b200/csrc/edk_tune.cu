@@ -59,11 +59,21 @@ edk_status time_apply(edk_operator* op, int dtype, const void* x, void* y, int64
 extern "C" edk_status edk_operator_configure(edk_operator* op, int32_t kernel, int32_t tps,
                                              int32_t block) {
   EDK_CHECK_ARG(op != nullptr, "edk_operator_configure: NULL operator");
-  EDK_CHECK_ARG(kernel == EDK_KERNEL_FAST || kernel == EDK_KERNEL_GENERIC,
-                "edk_operator_configure: kernel must be EDK_KERNEL_FAST or EDK_KERNEL_GENERIC");
+  EDK_CHECK_ARG(kernel >= EDK_KERNEL_FAST && kernel <= EDK_KERNEL_MATERIALIZED_STAGED,
+                "edk_operator_configure: unknown kernel");
   EDK_CHECK_ARG(tps == 1 || tps == 2 || tps == 4,
                 "edk_operator_configure: threads per state must be 1, 2 or 4");
   std::lock_guard<std::mutex> lk(op->mu);
+  if (kernel == EDK_KERNEL_MATERIALIZED || kernel == EDK_KERNEL_MATERIALIZED_STAGED) {
+    if (!op->sell_ok || (kernel == EDK_KERNEL_MATERIALIZED_STAGED && !op->sell_tma_ok)) {
+      set_error("edk_operator_configure: that materialised kernel needs a materialised operator "
+                "(edk_operator_materialize) whose windows fit the shared-memory stages");
+      return EDK_UNSUPPORTED;
+    }
+    op->sell_tma = kernel == EDK_KERNEL_MATERIALIZED_STAGED;
+    op->use_block = block < 0 ? -1 : (block != 0);
+    return EDK_OK;
+  }
   if (kernel == EDK_KERNEL_FAST && !(op->ff_ok && op->gather)) {
     set_error("edk_operator_configure: the fast kernel does not apply to this operator");
     return EDK_UNSUPPORTED;
@@ -120,6 +130,7 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
   if ((flags & EDK_TUNE_MATERIALIZE) || was_mat) {
     cands.push_back({EDK_KERNEL_MATERIALIZED, 0, 1, 0});
     if (multi) cands.push_back({EDK_KERNEL_MATERIALIZED, 0, 1, 1});
+    else cands.push_back({EDK_KERNEL_MATERIALIZED_STAGED, 0, 1, 0});
   }
 
   const int reps = 7;
@@ -128,8 +139,11 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
   edk_status rc = EDK_OK;
   for (const Cand& c : cands) {
     double ms = -1.0;
-    if (c.kernel == EDK_KERNEL_MATERIALIZED) {
+    const bool matk = c.kernel == EDK_KERNEL_MATERIALIZED || c.kernel == EDK_KERNEL_MATERIALIZED_STAGED;
+    if (matk) {
       if (edk_operator_materialize(op, 1, nullptr) != EDK_OK) continue;  // not materialisable
+      if (c.kernel == EDK_KERNEL_MATERIALIZED_STAGED && !op->sell_tma_ok) continue;
+      op->sell_tma = c.kernel == EDK_KERNEL_MATERIALIZED_STAGED;
     } else {
       if (op->sell_ok) edk_operator_materialize(op, 0, nullptr);
       edk_basis_set_search(b, c.search);
@@ -151,17 +165,22 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
       ++out.ncand;
     }
     if (ms < best) { best = ms; pick = c; }
-    if (c.kernel != EDK_KERNEL_MATERIALIZED && ms < best_free) { best_free = ms; pick_free = c; }
+    if (!matk && ms < best_free) { best_free = ms; pick_free = c; }
   }
   if (rc != EDK_OK) return rc;
   // install the fastest matrix-free choice (it also serves whenever the
   // materialised matrix is cleared), then the matrix if that wins
-  if (op->sell_ok && pick.kernel != EDK_KERNEL_MATERIALIZED) edk_operator_materialize(op, 0, nullptr);
+  const bool pick_mat =
+      pick.kernel == EDK_KERNEL_MATERIALIZED || pick.kernel == EDK_KERNEL_MATERIALIZED_STAGED;
+  if (op->sell_ok && !pick_mat) edk_operator_materialize(op, 0, nullptr);
   if (has_search) edk_basis_set_search(b, pick_free.search);
   op->use_ff = pick_free.kernel == EDK_KERNEL_FAST;
   op->tps = pick_free.tps;
-  op->use_block = multi ? (pick.kernel == EDK_KERNEL_MATERIALIZED ? pick : pick_free).block : -1;
-  if (pick.kernel == EDK_KERNEL_MATERIALIZED) EDK_RETURN_IF(edk_operator_materialize(op, 1, nullptr));
+  op->use_block = multi ? (pick_mat ? pick : pick_free).block : -1;
+  if (pick_mat) {
+    EDK_RETURN_IF(edk_operator_materialize(op, 1, nullptr));
+    op->sell_tma = pick.kernel == EDK_KERNEL_MATERIALIZED_STAGED;
+  }
   out.kernel = pick.kernel;
   out.search = b->dev.search ? EDK_SEARCH_SORTED : EDK_SEARCH_HASH;
   out.tps = pick_free.tps;

@@ -293,7 +293,7 @@ class Operator:
         E.check(E.load().edk_operator_materialize(self._h, 0, None))
         self.materialized = False
 
-    _KERNELS = {"fast": 0, "generic": 1, "materialized": 2}
+    _KERNELS = {"fast": 0, "generic": 1, "materialized": 2, "materialized_staged": 3}
 
     def configure_(self, kernel="fast", tps=1, block=None):
         """Pick the matrix-free kernel by hand: "fast" (bond families, `tps`
@@ -314,7 +314,7 @@ class Operator:
                                                 C.byref(r)))
         names = {v: k for k, v in self._KERNELS.items()}
         srch = {0: "hash", 1: "sorted"}
-        self.materialized = r.kernel == E.KERNEL_MATERIALIZED
+        self.materialized = r.kernel in (E.KERNEL_MATERIALIZED, E.KERNEL_MATERIALIZED_STAGED)
         return {"kernel": names[r.kernel], "search": srch[r.search], "tps": r.tps,
                 "block": bool(r.block), "ms": r.ms,
                 "candidates": [(names[r.cand_kernel[i]], srch[r.cand_search[i]], r.cand_tps[i],

@@ -208,12 +208,15 @@ edk_status edk_block_lanczos(int32_t nops, edk_operator* const* ops,
  * (each nonzero located once for all columns, as colmn! does,
  * Operator.jl:417-465); block = 0 runs them one column at a time; block = -1
  * (the default) uses the SpMM matrix-free and the columns on a materialised
- * matrix.  Every
+ * matrix.  On a materialised operator, EDK_KERNEL_MATERIALIZED /
+ * EDK_KERNEL_MATERIALIZED_STAGED select its plain or shared-memory-staged
+ * product (tps ignored).  Every
  * choice computes the same product as EDKit's mul! (Operator.jl:309-328).
  * No reference counterpart as a call: EDKit has one CPU kernel. */
 #define EDK_KERNEL_FAST 0
 #define EDK_KERNEL_GENERIC 1
 #define EDK_KERNEL_MATERIALIZED 2
+#define EDK_KERNEL_MATERIALIZED_STAGED 3  /* entries staged in shared memory by bulk copies */
 edk_status edk_operator_configure(edk_operator* op, int32_t kernel, int32_t tps, int32_t block);
 
 /* Autotuner: times every admissible (kernel, threads per state, index
