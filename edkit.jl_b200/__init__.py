@@ -7,13 +7,15 @@ include/edk.h); this package is the Python mirror of the reference's Julia API.
 from ._lib import EDKError, load as _load
 from .algorithms import (KrylovEvolutionDiagnostics, batch_lanczos_e0, block_lanczos, gapratio,
                          lanczos_e0, meangapratio, productstate, timeevolve, tridiag_eigen)
-from .basis import (AbelianBasis, AbstractBasis, ProjectedBasis, TensorBasis,
-                    TranslationalBasis, TranslationParityBasis, basis)
+from .basis import (AbelianBasis, AbstractBasis, FlipBasis, ParityBasis, ParityFlipBasis,
+                    ProjectedBasis, TensorBasis, TranslationalBasis, TranslationFlipBasis,
+                    TranslationParityBasis, basis)
 from .operator import Operator, mul, mul_, operator, spin, trans_inv_operator, σ
 
 __all__ = [
     "EDKError", "TensorBasis", "ProjectedBasis", "TranslationalBasis", "TranslationParityBasis",
-    "AbelianBasis", "AbstractBasis", "basis", "spin", "σ", "operator", "trans_inv_operator",
+    "AbelianBasis", "AbstractBasis", "ParityBasis", "FlipBasis", "ParityFlipBasis",
+    "TranslationFlipBasis", "basis", "spin", "σ", "operator", "trans_inv_operator",
     "Operator", "mul", "mul_", "lanczos_e0", "batch_lanczos_e0", "block_lanczos", "timeevolve",
     "tridiag_eigen", "gapratio", "meangapratio", "productstate", "KrylovEvolutionDiagnostics", "version",
 ]

@@ -17,7 +17,7 @@ OK, INVALID_ARG, NOT_HERMITIAN, OOM, CUDA_ERROR, TIMEOUT, NOT_CONVERGED, UNSUPPO
 # edk_dtype
 F64, C128, F32, C64 = range(4)
 HOST, DEVICE = 0, 1
-TENSOR, PROJECTED, TRANSLATIONAL, TRANSPARITY, ABELIAN = range(5)
+TENSOR, PROJECTED, TRANSLATIONAL, TRANSPARITY, ABELIAN, TRANSFLIP = range(6)
 PREC_FP64, PREC_MIXED = 0, 1
 
 EXPORTS = [

@@ -243,6 +243,7 @@ def _compute_period(perm, inv):
 
 class AbelianBasis(AbstractBasis):
     kind = E.ABELIAN
+    _desc_kind = E.ABELIAN
 
     def __init__(self, *, L, gens, N=None, f=None, base=2, vectorized=False):
         orders = np.array([g[0] for g in gens], dtype=np.int32)
@@ -261,7 +262,7 @@ class AbelianBasis(AbstractBasis):
                     g = (lambda d: (int(np.sum(d)) == num) and (f(d) if f else True))
             if g is not None:
                 allow = _allow_bitmap(g, L, vectorized)
-        d = _desc(E.ABELIAN, L, base, N=N if use_gosper else None, allow=allow)
+        d = _desc(self._desc_kind, L, base, N=N if use_gosper else None, allow=allow)
         d.ngen = len(gens)
         d.gen_order = orders.ctypes.data
         d.gen_q = qs.ctypes.data
@@ -301,6 +302,115 @@ def basis(dtype=None, *, L, f=None, base=2, N=None, k=None, a=1, p=None, z=None,
             return TensorBasis(L=L, base=base)
         return ProjectedBasis(L=L, f=f, N=N, base=base, vectorized=vectorized)
     return AbelianBasis(L=L, gens=gens, N=N, f=f, base=base, vectorized=vectorized)
+
+
+# ---------------------------------------------------------------------------
+# The reference's dedicated symmetry bases.  Each is the AbelianBasis of its
+# generators — reflection P, spin flip Z, translation T^a — and shares its
+# conventions exactly: representative = the orbit minimum, norm
+# R = sqrt(|G| * n_stab) (ParityBasis/FlipBasis: sqrt 2, or 2 on a fixed
+# point; ParityFlipBasis: 2, 2 sqrt 2, 4; TranslationFlipBasis:
+# 2len/sqrt(p) [/sqrt 2]), index coefficient = the character of the first
+# group element (in P, Z or T-then-Z order) reaching the minimum times R.
+# Their charge N counts zeros, as in the reference (sum(dgt) == L - N), and f
+# is honoured together with N.
+# ---------------------------------------------------------------------------
+def _charge_kwargs(L, N, f, vectorized):
+    if N is not None and not 0 <= N <= L:
+        raise ValueError(f"N = {N} out of range for L = {L}")
+    if f is None:
+        return dict(N=None if N is None else L - N)  # set bits on the device path
+    if N is None:
+        return dict(f=f, vectorized=vectorized)
+    num = L - N
+    if vectorized:
+        return dict(f=lambda d: (d.sum(axis=1) == num) & np.asarray(f(d), bool),
+                    vectorized=True)
+    return dict(f=lambda d: int(np.sum(d)) == num and bool(f(d)), vectorized=False)
+
+
+def _reflection(L):
+    return (2, None, [L - i + 1 for i in range(1, L + 1)], [0] * L)
+
+
+def _flip(L):
+    return (2, None, list(range(1, L + 1)), [1] * L)
+
+
+def _z2(gen, sign):
+    if sign not in (1, -1):
+        raise ValueError("Invalid parity")
+    return (gen[0], 1 if sign == -1 else 0, gen[2], gen[3])
+
+
+class ParityBasis(AbelianBasis):
+    """ParityBasis (src/Basis/ParityBasis.jl:14-90, index :109-121): reflection
+    parity p = +-1."""
+
+    def __init__(self, dtype=None, *, L, p, f=None, N=None, base=2, vectorized=False, **_):
+        if base != 2:
+            raise ValueError("the GPU path supports base 2 (spin-1/2) only")
+        super().__init__(L=L, gens=[_z2(_reflection(L), p)], **_charge_kwargs(L, N, f, vectorized))
+        self.P = p
+
+    def eltype(self):
+        return np.float64
+
+
+class FlipBasis(AbelianBasis):
+    """FlipBasis (src/Basis/FlipBasis.jl:40-95, index :105-115): spin-flip
+    eigenvalue p = +-1; with N only the half-filled sector (2N = L)."""
+
+    def __init__(self, dtype=None, *, L, p, f=None, N=None, base=2, vectorized=False, **_):
+        if base != 2:
+            raise ValueError("the GPU path supports base 2 (spin-1/2) only")
+        if N is not None and 2 * N != L:
+            raise ValueError(f"N = {N} not compatible.")
+        super().__init__(L=L, gens=[_z2(_flip(L), p)], **_charge_kwargs(L, N, f, vectorized))
+        self.P = p
+
+    def eltype(self):
+        return np.float64
+
+
+class ParityFlipBasis(AbelianBasis):
+    """ParityFlipBasis (src/Basis/ParityFlipBasis.jl:37-94, index :104-125):
+    reflection parity p and spin flip z, both +-1."""
+
+    def __init__(self, dtype=None, *, L, p, z, f=None, N=None, base=2, vectorized=False, **_):
+        if base != 2:
+            raise ValueError("the GPU path supports base 2 (spin-1/2) only")
+        if N is not None and 2 * N != L:
+            raise ValueError(f"N = {N} not compatible.")
+        super().__init__(L=L, gens=[_z2(_reflection(L), p), _z2(_flip(L), z)],
+                         **_charge_kwargs(L, N, f, vectorized))
+        self.P, self.Z = p, z
+
+    def eltype(self):
+        return np.float64
+
+
+class TranslationFlipBasis(AbelianBasis):
+    """TranslationFlipBasis (src/Basis/TranslationalFlipBasis.jl:50-156, index
+    :172-213): momentum k with unit cell a, spin-flip eigenvalue p; its norms
+    are the reference's 2len/sqrt(period) [/sqrt 2] expressions."""
+
+    _desc_kind = E.TRANSFLIP
+
+    def __init__(self, dtype=None, *, L, k=0, p=1, f=None, N=None, a=1, base=2,
+                 vectorized=False, **_):
+        if base != 2:
+            raise ValueError("the GPU path supports base 2 (spin-1/2) only")
+        if L % a:
+            raise ValueError(f"Length of unit-cell {a} incompatible with L={L}")
+        if N is not None and 2 * N != L:
+            raise ValueError(f"N = {N} not compatible.")
+        # the generator below rotates against the reference's circshift!, so
+        # its quantum number is -k (phases exp(-i 2pi k' n / len), k' = mod(-k, len))
+        perm = [((i - a - 1) % L) + 1 for i in range(1, L + 1)]
+        super().__init__(L=L, gens=[(L // a, (-k) % (L // a), perm, [0] * L), _z2(_flip(L), p)],
+                         **_charge_kwargs(L, N, f, vectorized))
+        self.K, self.P, self.A = k, p, a
 
 
 def binomial(n, k):

@@ -33,6 +33,7 @@ struct BuildParams {
   int L, A, len;
   int Kmom;        // mod(-k, len) for TranslationalBasis
   int Kpar;        // +-1 for TranslationParityBasis
+  int pairnorm;    // abelian (translation, Z2) group with TranslationFlipBasis norms
   int P;           // parity
   int full;        // 1: candidates are all 2^L states; 0: fixed popcount K
   int K;           // popcount of candidates
@@ -140,6 +141,41 @@ __device__ inline int judge_abelian(S s0, const BuildParams& p) {
   return N;
 }
 
+// The same check for the (translation, flip) pair, returning the norm-table
+// index of TranslationFlipBasis (TranslationalFlipBasis.jl:50-91): 1 +
+// (Qp ? len + R - 1 : R - 1) with R the translation period and Qp whether a
+// flipped translate returns the state.
+template <class S>
+__device__ inline int judge_abelian_pair(S s0, const BuildParams& p) {
+  S mask = (S)p.maskL;
+  int cnt[kMaxGen];
+  for (int g = 0; g < kMaxGen; ++g) cnt[g] = 0;
+  const int len = p.gens[0].order;
+  const int64_t order = (int64_t)len * p.gens[1].order;
+  S cur = s0;
+  int R = len;
+  bool Qp = false;
+  for (int64_t t = 2; t <= order; ++t) {
+    for (int g = 0; g < p.ngen; ++g) {
+      cur = apply_gen(p.gens[g], cur, p.L, mask);
+      if (++cnt[g] >= p.gens[g].order) cnt[g] = 0; else break;
+    }
+    if (cur < s0) return 0;
+    if (cur == s0) {
+      double pr = 1.0, pi = 0.0;
+      for (int g = 0; g < p.ngen; ++g) {
+        double2 c = p.gphase[p.gens[g].phase_off + cnt[g]];
+        double nr = pr * c.x - pi * c.y, ni = pr * c.y + pi * c.x;
+        pr = nr; pi = ni;
+      }
+      if (!(hypot(pr - 1.0, pi) < 1e-14)) return 0;
+      if (cnt[1] == 0) R = min(R, cnt[0]);
+      else Qp = true;
+    }
+  }
+  return 1 + (Qp ? len + R - 1 : R - 1);
+}
+
 template <class S>
 __device__ inline int judge(S s, const BuildParams& p) {
   if (p.allow && !((p.allow[(uint64_t)s >> 6] >> ((uint64_t)s & 63)) & 1ull)) return 0;
@@ -147,7 +183,7 @@ __device__ inline int judge(S s, const BuildParams& p) {
     case EDK_PROJECTED: return 1;
     case EDK_TRANSLATIONAL: return judge_trans(s, p);
     case EDK_TRANSPARITY: return judge_transpar(s, p);
-    default: return judge_abelian(s, p);
+    default: return p.pairnorm ? judge_abelian_pair(s, p) : judge_abelian(s, p);
   }
 }
 
@@ -345,7 +381,13 @@ bool compile_perm(const std::vector<int>& perm, int L, GenDev& g) {
 
 edk_status validate_desc(const edk_basis_desc* d) {
   EDK_CHECK_ARG(d != nullptr, "edk_basis_create: desc is NULL");
-  EDK_CHECK_ARG(d->kind >= EDK_TENSOR && d->kind <= EDK_ABELIAN, "edk_basis_create: bad kind");
+  EDK_CHECK_ARG(d->kind >= EDK_TENSOR && d->kind <= EDK_TRANSFLIP, "edk_basis_create: bad kind");
+  if (d->kind == EDK_TRANSFLIP) {
+    EDK_CHECK_ARG(d->ngen == 2 && d->gen_order && d->gen_q && d->gen_perm && d->gen_inv,
+                  "edk_basis_create: TranslationFlipBasis takes two generators (T^a, flip)");
+    EDK_CHECK_ARG(d->gen_order[1] == 2 && d->gen_order[0] >= 1,
+                  "edk_basis_create: TranslationFlipBasis generators: translation, then flip");
+  }
   EDK_CHECK_ARG(d->L >= 1, "edk_basis_create: L must be >= 1");
   if (d->base != 2) {
     set_error("edk_basis_create: the GPU path supports base 2 (spin-1/2) only");
@@ -469,7 +511,17 @@ static edk_status gpu_build(edk_basis* b, const edk_basis_desc& d, cudaStream_t 
       set_error("edk_basis_create: abelian group order above 128 is not supported");
       return EDK_UNSUPPORTED;
     }
-    for (int64_t i = 1; i <= Ng; ++i) ntab.push_back((Ng % i == 0) ? std::sqrt((double)(Ng * i)) : 0.0);
+    if (b->pairnorm) {  // TranslationFlipBasis: vcat(N1, N2), N2 = 2len/sqrt(i), N1 = N2/sqrt(2)
+      const int len = b->gen_order[0];
+      std::vector<double> n2(len);
+      for (int i = 1; i <= len; ++i) n2[i - 1] = (double)(2 * len) / std::sqrt((double)i);
+      for (int i = 0; i < len; ++i) ntab.push_back(n2[i] / std::sqrt(2.0));
+      for (int i = 0; i < len; ++i) ntab.push_back(n2[i]);
+      p.pairnorm = 1;
+    } else {
+      for (int64_t i = 1; i <= Ng; ++i)
+        ntab.push_back((Ng % i == 0) ? std::sqrt((double)(Ng * i)) : 0.0);
+    }
     p.ngen = (int)b->gens_host.size();
     p.gens = b->gens.as<GenDev>();
     p.gphase = b->phase.as<double2>();
@@ -615,7 +667,10 @@ extern "C" edk_status edk_basis_create(const edk_basis_desc* desc, edk_basis** o
   auto* b = new edk_basis;
   std::unique_ptr<edk_basis> guard(b);
   b->desc = *desc;
-  b->kind = desc->kind;
+  // TranslationFlipBasis: the generic symmetry-group path with its own norms
+  b->pairnorm = desc->kind == EDK_TRANSFLIP;
+  b->kind = b->pairnorm ? (int)EDK_ABELIAN : desc->kind;
+  b->desc.kind = b->kind;
   b->L = desc->L;
   b->A = (desc->kind == EDK_TRANSLATIONAL || desc->kind == EDK_TRANSPARITY) ? desc->a : 1;
   b->len = b->L / b->A;

@@ -261,6 +261,7 @@ struct edk_basis {
   std::vector<std::vector<int>> gen_perm;
   std::vector<std::vector<uint8_t>> gen_inv;
   bool phase_complex = false;
+  bool pairnorm = false;  // TranslationFlipBasis norms on the abelian path
   int device = 0;  // CUDA device the tables live on
   cudaStream_t stream = nullptr;
   std::mutex mu;

@@ -52,7 +52,13 @@ typedef enum {
   EDK_PROJECTED = 1,     /* ProjectedBasis         src/Basis/ProjectedBasis.jl:14-260 */
   EDK_TRANSLATIONAL = 2, /* TranslationalBasis     src/Basis/TranslationalBasis.jl:22-349 */
   EDK_TRANSPARITY = 3,   /* TranslationParityBasis src/Basis/TranslationalParityBasis.jl:15-241 */
-  EDK_ABELIAN = 4        /* AbelianBasis / basis() src/Basis/AbelianBasis.jl:498-847 */
+  EDK_ABELIAN = 4,       /* AbelianBasis / basis() src/Basis/AbelianBasis.jl:498-847 */
+  EDK_TRANSFLIP = 5      /* TranslationFlipBasis   src/Basis/TranslationalFlipBasis.jl:9-213:
+                            generators as for EDK_ABELIAN, exactly two — translation by a
+                            (order L/a, q = -k mod L/a: the generator rotates against the
+                            reference's circshift!) then spin flip (order 2, q = 0 for
+                            p = +1, 1 for p = -1) — with the reference's norms
+                            2len/sqrt(period) [/sqrt 2 without a flip match] */
 } edk_basis_kind;
 
 typedef struct edk_basis edk_basis;

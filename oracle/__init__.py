@@ -310,6 +310,231 @@ def basis(L, N=None, k=None, a=1, p=None, z=None, symmetries=None, f=None, base=
 # ---------------------------------------------------------------------------
 # Operator application
 # ---------------------------------------------------------------------------
+# ---------------------------------------------------------------------------
+# Dedicated Z2 / translation+flip bases, restated in plain Python from the
+# reference (small L only: every one of the base^L states is judged).
+# Each returns (I 1-based ascending, R) and an index(state) -> (coeff, pos)
+# following the reference's own index function.
+# ---------------------------------------------------------------------------
+def _dgt(s, L):
+    return [(s >> (L - 1 - q)) & 1 for q in range(L)]
+
+
+def _rev(s, L):  # _int_reverse, AbstractBasis.jl:417-425 (base 2)
+    return int(format(s, f"0{L}b")[::-1], 2)
+
+
+def _bsearch(I, x):  # binary_search, ProjectedBasis.jl:71-81 (0 when absent)
+    import bisect
+    j = bisect.bisect_left(I, x)
+    return j + 1 if j < len(I) and I[j] == x else 0
+
+
+def _charge_ok(dgt, L, N, f):
+    if f is not None and not f(np.array(dgt)):
+        return False
+    return N is None or sum(dgt) == L - N  # EDKit digit convention
+
+
+class DedicatedBasis:
+    def __init__(self, L, I, R, index_fn):
+        self.L, self.I, self.R, self._index = L, I, R, index_fn
+        self.dim = len(I)
+
+    def index_state(self, s):
+        return self._index(self, s)
+
+
+def parity_basis(L, p, N=None, f=None):
+    """ParityBasis: judge ParityBasis.jl:40-57, index :109-121."""
+    I, R = [], []
+    for s in range(2 ** L):
+        dgt = _dgt(s, L)
+        if not _charge_ok(dgt, L, N, f):
+            continue
+        i, In = s + 1, _rev(s, L) + 1
+        if In < i:
+            continue
+        if In == i:
+            if p != 1:
+                continue
+            R.append(2.0)
+        else:
+            R.append(math.sqrt(2))
+        I.append(i)
+
+    def index(b, s):
+        Ia, Ib = s + 1, _rev(s, L) + 1
+        i, n = (_bsearch(b.I, Ib), p) if Ib < Ia else (_bsearch(b.I, Ia), 1)
+        return (0.0, 1) if i == 0 else (n * b.R[i - 1], i)
+    return DedicatedBasis(L, I, R, index)
+
+
+def flip_basis(L, p, N=None, f=None):
+    """FlipBasis: judge FlipBasis.jl:40-55 (partner MAX - i), index :105-115."""
+    MAX = 2 ** L + 1
+    I, R = [], []
+    for s in range(2 ** L):
+        dgt = _dgt(s, L)
+        if not _charge_ok(dgt, L, N, f):
+            continue
+        i = s + 1
+        In = MAX - i
+        if In < i:
+            continue
+        if In == i:
+            if p != 1:
+                continue
+            R.append(2.0)
+        else:
+            R.append(math.sqrt(2))
+        I.append(i)
+
+    def index(b, s):
+        Ia = s + 1
+        Ib = MAX - Ia
+        i, n = (_bsearch(b.I, Ib), p) if Ib < Ia else (_bsearch(b.I, Ia), 1)
+        return (0.0, 1) if i == 0 else (n * b.R[i - 1], i)
+    return DedicatedBasis(L, I, R, index)
+
+
+def parityflip_basis(L, p, z, N=None, f=None):
+    """ParityFlipBasis: double_parity_check ParityFlipBasis.jl:37-55 with the
+    norm table [2, 2sqrt(2), 0, 4], index :104-125."""
+    MAX = 2 ** L + 1
+    C = [2.0, 2 * math.sqrt(2), 0.0, 4.0]
+    I, R = [], []
+    for s in range(2 ** L):
+        dgt = _dgt(s, L)
+        if not _charge_ok(dgt, L, N, f):
+            continue
+        i = s + 1
+        Ip = _rev(s, L) + 1
+        if Ip < i:
+            continue
+        Iz = MAX - i
+        if Iz < i:
+            continue
+        Ipz = MAX - Ip
+        if Ipz < i:
+            continue
+        n = 1
+        if Ip == i:
+            if p != 1:
+                continue
+            n += 1
+        if Iz == i:
+            if z != 1:
+                continue
+            n += 1
+        if Ipz == i:
+            if p * z != 1:
+                continue
+            n += 1
+        I.append(i)
+        R.append(C[n - 1])
+
+    def index(b, s):
+        I0 = s + 1
+        Ip = _rev(s, L) + 1
+        Iz = (2 ** L - 1 - s) + 1
+        Ipz = (2 ** L - 1 - (Ip - 1)) + 1
+        Ir = min(I0, Iz, Ip, Ipz)
+        i = _bsearch(b.I, Ir)
+        if i == 0:
+            return (0.0, 1)
+        r = b.R[i - 1]
+        if Ir == I0:
+            return (r, i)
+        if Ir == Ip:
+            return (p * r, i)
+        if Ir == Iz:
+            return (z * r, i)
+        return (p * z * r, i)
+    return DedicatedBasis(L, I, R, index)
+
+
+def _phase_factor(k, length):  # TranslationalBasis.jl:277-285
+    if k == 0:
+        return [1.0] * length
+    if 2 * k == length:
+        return [1.0 if i % 2 == 0 else -1.0 for i in range(length)]
+    return [complex(math.cos(-2 * math.pi / length * k * i), math.sin(-2 * math.pi / length * k * i))
+            for i in range(length)]
+
+
+def transflip_basis(L, k=0, p=1, N=None, a=1, f=None):
+    """TranslationFlipBasis: judge TranslationalFlipBasis.jl:50-91 (norms
+    vcat(N1, N2), N2 = 2len/sqrt(i), N1 = N2/sqrt 2), index :132-171."""
+    length = L // a
+    K = (-k) % length
+    MAX = 2 ** L + 1
+    N2 = [2 * length / math.sqrt(i) for i in range(1, length + 1)]
+    N1 = [x / math.sqrt(2) for x in N2]
+    Ctab = N1 + N2
+    mask = (1 << L) - 1
+    I, R = [], []
+    for s in range(2 ** L):
+        dgt = _dgt(s, L)
+        if not _charge_ok(dgt, L, N, f):
+            continue
+        i = s + 1
+        Rr, Qp = length, False
+        In = MAX - i
+        if In < i:
+            continue
+        if In == i:
+            Qp = True
+            if p != 1:
+                continue
+        ok = True
+        st = s
+        for n in range(1, length):
+            st = ((st >> a) | (st << (L - a))) & mask  # circshift!(dgt, a): digits move right
+            In1 = st + 1
+            In2 = MAX - In1
+            if In1 < i or In2 < i:
+                ok = False
+                break
+            if In2 == i:
+                if (p == 1) != ((n * K) // (length // 2) % 2 == 0):
+                    ok = False
+                    break
+                Qp = True
+            if In1 == i:
+                if (n * K) % length != 0:
+                    ok = False
+                    break
+                Rr = n
+                break
+        if not ok:
+            continue
+        I.append(i)
+        R.append(Ctab[length + Rr - 1] if Qp else Ctab[Rr - 1])
+    Cph = _phase_factor(K, length)
+
+    def index(b, s):  # one loop over rotations, both minima, first strict
+        Ia0 = s + 1
+        Iam, Rm, Ibm, M = Ia0, 0, (2 ** L - 1 - s) + 1, 0
+        st = s
+        for i in range(1, length):
+            st = ((st >> a) | (st << (L - a))) & mask
+            Ia1 = st + 1
+            if Ia1 == Ia0:
+                break
+            if Ia1 < Iam:
+                Iam, Rm = Ia1, i
+            Ib1 = (2 ** L - 1 - st) + 1
+            if Ib1 < Ibm:
+                Ibm, M = Ib1, i
+        if Ibm < Iam:
+            i, n = _bsearch(b.I, Ibm), p * Cph[M]
+        else:
+            i, n = _bsearch(b.I, Iam), Cph[Rm]
+        return (0.0, 1) if i == 0 else (n * b.R[i - 1], i)
+    return DedicatedBasis(L, I, R, index)
+
+
 class OOperator:
     """Operator{Tv,Tb}: merged local terms + basis (Operator.jl:24-28)."""
 

@@ -292,3 +292,30 @@ def test_lanczos_cgs2_e0_matches_dense(O):
     v0 = np.random.default_rng(5).standard_normal(B.dim)
     ev, a, b = O.lanczos_e0(lambda v: Hd @ v, v0, min(B.dim, 60))
     assert abs(ev[0] - np.linalg.eigvalsh(Hd)[0]) < 1e-10
+
+
+def test_dedicated_basis_restatements_sector_sizes(O):
+    """EigenvalueTest.jl:240-330, 562-575: the sectors of ParityBasis (with the
+    PXP predicate and with N), ParityFlipBasis and TranslationFlipBasis add up
+    to the unreduced space, as the reference's own tests require."""
+    import math
+
+    def pxp(v):
+        return all(v[i] == 0 or v[(i + 1) % len(v)] == 0 for i in range(len(v)))
+    for L in range(3, 11):
+        full = O.projected(L, f=pxp).dim
+        assert sum(O.parity_basis(L, p, f=pxp).dim for p in (1, -1)) == full
+    for L in range(2, 9):
+        for n in range(L + 1):
+            assert sum(O.parity_basis(L, p, N=n).dim for p in (1, -1)) == math.comb(L, n)
+    for L in range(2, 9):
+        assert sum(O.parityflip_basis(L, p, z).dim for p in (1, -1) for z in (1, -1)) == 2 ** L
+        assert sum(O.flip_basis(L, p).dim for p in (1, -1)) == 2 ** L
+    for L in range(4, 11, 2):
+        for k in range(L):
+            assert sum(O.transflip_basis(L, k, p).dim for p in (1, -1)) == \
+                O.translational(L, k=k).dim
+    # norms: fixed points of the reflection get 2, pairs sqrt 2 (ParityBasis.jl:47-55)
+    b = O.parity_basis(4, 1)
+    pal = {int(format(i - 1, "04b")[::-1], 2) == i - 1 for i in b.I}
+    assert set(b.R) <= {2.0, math.sqrt(2)} and len(pal) == 2
