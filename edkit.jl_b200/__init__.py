@@ -6,7 +6,8 @@ include/edk.h); this package is the Python mirror of the reference's Julia API.
 """
 from ._lib import EDKError, load as _load
 from .algorithms import (KrylovEvolutionDiagnostics, batch_lanczos_e0, block_lanczos, gapratio,
-                         lanczos_e0, meangapratio, productstate, timeevolve, tridiag_eigen)
+                         ground_state, lanczos_e0, meangapratio, productstate, timeevolve,
+                         tridiag_eigen)
 from .basis import (AbelianBasis, AbstractBasis, FlipBasis, ParityBasis, ParityFlipBasis,
                     ProjectedBasis, TensorBasis, TranslationalBasis, TranslationFlipBasis,
                     TranslationParityBasis, basis)
@@ -16,7 +17,8 @@ __all__ = [
     "EDKError", "TensorBasis", "ProjectedBasis", "TranslationalBasis", "TranslationParityBasis",
     "AbelianBasis", "AbstractBasis", "ParityBasis", "FlipBasis", "ParityFlipBasis",
     "TranslationFlipBasis", "basis", "spin", "σ", "operator", "trans_inv_operator",
-    "Operator", "mul", "mul_", "lanczos_e0", "batch_lanczos_e0", "block_lanczos", "timeevolve",
+    "Operator", "mul", "mul_", "lanczos_e0", "ground_state", "batch_lanczos_e0", "block_lanczos",
+    "timeevolve",
     "tridiag_eigen", "gapratio", "meangapratio", "productstate", "KrylovEvolutionDiagnostics", "version",
 ]
 

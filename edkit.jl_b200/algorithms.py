@@ -60,6 +60,26 @@ def lanczos_e0(H: Operator, v0=None, *, m=300, nev=1, tol=0.0, check_every=10,
     return ev, info
 
 
+def ground_state(H: Operator, v0=None, *, m=300, tol=1e-12, check_every=10, precision="fp64",
+                 refine_steps=20, complex_vectors=False, seed=0):
+    """(E0, psi): the lowest eigenvalue and its normalised Lanczos Ritz vector
+    (FP64; complex when H or v0 is).  Same run as lanczos_e0."""
+    D = H.size(1)
+    if v0 is None:
+        v0 = np.random.default_rng(seed).standard_normal(D)
+    dt = E.C128 if np.iscomplexobj(v0) else E.F64
+    v0 = np.ascontiguousarray(v0, dtype=np.complex128 if dt == E.C128 else np.float64)
+    cx = H.is_complex or complex_vectors or dt == E.C128
+    psi = np.zeros(D, dtype=np.complex128 if cx else np.float64)
+    o = _opts(m, 1, tol, check_every, precision, refine_steps, True, complex_vectors)
+    ev = np.zeros(1)
+    d = E.LanczosDiag()
+    E.check(E.load().edk_lanczos_ground_state(H._h, C.byref(o), E.ptr(v0), dt, E.HOST,
+                                              E.ptr(ev), E.ptr(psi),
+                                              E.C128 if cx else E.F64, C.byref(d)))
+    return float(ev[0]), psi, _diag_dict(d)
+
+
 def batch_lanczos_e0(ops, v0s=None, *, m=200, nev=1, tol=0.0, check_every=10, precision="fp64",
                      refine_steps=20, reorth=True, seed=0):
     """Lanczos over many independent operators (sectors / instances)."""

@@ -768,7 +768,7 @@ __global__ void k_cast(const S* __restrict__ src, int64_t n, D* __restrict__ dst
 // Group-level driver: FP64 or mixed (FP32 Krylov vectors + FP64 refinement).
 edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczos_opts& o,
                          const void* v0_dev, int v0_dt, cudaStream_t st,
-                         std::vector<OpResult>& res, edk_lanczos_diag* diag) {
+                         std::vector<OpResult>& res, edk_lanczos_diag* diag, void* ritz_out) {
   double t0 = wall();
   const int nops = (int)ops.size();
   bool cx = o.complex_vectors != 0 || v0_dt == EDK_C128 || v0_dt == EDK_C64;
@@ -830,6 +830,10 @@ edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczo
     }
   int steps_low = 0, mvs = 0, bd = 0;
   for (auto& r : res) { steps_low = std::max(steps_low, r.steps); mvs += r.steps; bd |= r.status == 2; }
+  // global element offset of each operator in the concatenated layout
+  std::vector<int64_t> goff(nops);
+  for (int q = 0; q < nops; ++q) goff[q] = E.hops[q].woff;
+  if (!mixed && ritz_out) EDK_RETURN_IF(ritz_vectors(E, res, ritz_out, 1));
   if (mixed) {
     // FP64 refinement restarted from the sum of the nev lowest Ritz vectors.
     // A single eigenvalue converges in a few steps from its FP32 Ritz vector;
@@ -867,6 +871,22 @@ edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczo
           next.push_back(q);
           keep.push_back((int)i);
         }
+      }
+      if (ritz_out) {
+        // lowest Ritz vectors of the operators this round finalises
+        DevBuf gs;
+        EDK_RETURN_IF(gs.alloc_async((size_t)F.totalD * esz(wdt), st));
+        EDK_RETURN_IF(ritz_vectors(F, r2, gs.p, 1));
+        size_t k = 0;
+        const bool last_round = round == 3;  // restarts end here: every vector is final
+        for (size_t i = 0; i < active.size(); ++i) {
+          if (!last_round && k < keep.size() && keep[k] == (int)i) { ++k; continue; }
+          const int q = active[i];
+          EDK_TRY_CUDA(cudaMemcpyAsync((char*)ritz_out + goff[q] * esz(wdt),
+                                       (char*)gs.p + F.hops[i].woff * esz(wdt),
+                                       (size_t)F.Ds[i] * esz(wdt), cudaMemcpyDeviceToDevice, st));
+        }
+        EDK_TRY_CUDA(cudaStreamSynchronize(st));
       }
       if (next.empty()) break;
       // Ritz vectors of this round (F's layout), then the restarted subset

@@ -327,9 +327,12 @@ struct OpResult {
   int steps = 0;
   int status = 0;  // 0 ran to the step limit, 1 converged, 2 breakdown, 3 zero norm
 };
+// ritz_out (optional, device): every operator's lowest Ritz vector in the
+// FP64 working dtype (F64 or C128), concatenated in operator order
 edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczos_opts& o,
                          const void* v0_dev, int v0_dt, cudaStream_t st,
-                         std::vector<OpResult>& res, edk_lanczos_diag* diag);
+                         std::vector<OpResult>& res, edk_lanczos_diag* diag,
+                         void* ritz_out = nullptr);
 // implemented in edk_util.cpp
 int tridiag_eigvals(int m, const double* a, const double* b, double* w);
 int tridiag_eigen(int m, const double* a, const double* b, double* w, double* Q);

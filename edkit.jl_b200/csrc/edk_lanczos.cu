@@ -520,10 +520,79 @@ static edk_status ritz_vector(Engine& E, const RunResult& R, void* out) {
 
 using namespace edk;
 
+// gs_out (optional, device, D elements of the FP64 working dtype): the lowest
+// Ritz vector, normalised
+static edk_status lanczos_common(edk_operator* op, const edk_lanczos_opts* opts, const void* v0,
+                                 int32_t v0_dtype, int32_t ptr_kind, double* evals,
+                                 double* alpha, double* beta, edk_lanczos_diag* diag,
+                                 void* gs_out);
+
 extern "C" edk_status edk_lanczos_e0(edk_operator* op, const edk_lanczos_opts* opts,
                                      const void* v0, int32_t v0_dtype, int32_t ptr_kind,
                                      double* evals, double* alpha, double* beta,
                                      edk_lanczos_diag* diag) {
+  return lanczos_common(op, opts, v0, v0_dtype, ptr_kind, evals, alpha, beta, diag, nullptr);
+}
+
+namespace edk {
+namespace gs_detail {
+template <class T>
+__global__ void k_sumsq(const T* __restrict__ v, int64_t n, double* __restrict__ out) {
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    acc += (double)v[i] * (double)v[i];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+__global__ void k_scale_d(double* __restrict__ v, int64_t n, const double* __restrict__ ss) {
+  const double s = 1.0 / sqrt(*ss);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v[i] *= s;
+}
+}  // namespace gs_detail
+}  // namespace edk
+
+extern "C" edk_status edk_lanczos_ground_state(edk_operator* op, const edk_lanczos_opts* opts,
+                                               const void* v0, int32_t v0_dtype,
+                                               int32_t ptr_kind, double* evals, void* psi,
+                                               int32_t psi_dtype, edk_lanczos_diag* diag) {
+  EDK_CHECK_ARG(op && opts && v0 && evals && psi, "edk_lanczos_ground_state: NULL argument");
+  EDK_CHECK_ARG(v0_dtype >= EDK_F64 && v0_dtype <= EDK_C64, "edk_lanczos_ground_state: bad v0 dtype");
+  const bool cx = op->is_complex || opts->complex_vectors || is_cx(v0_dtype);
+  const int wdt = cx ? EDK_C128 : EDK_F64;
+  if (psi_dtype != wdt) {
+    set_error(cx ? "edk_lanczos_ground_state: the ground state is complex here; psi must be EDK_C128"
+                 : "edk_lanczos_ground_state: the ground state is real here; psi must be EDK_F64");
+    return EDK_INVALID_ARG;
+  }
+  const int64_t D = op->b->D;
+  EDK_CHECK_ARG(D >= 1, "edk_lanczos_ground_state: empty basis");
+  DevBuf gs, ss;
+  EDK_RETURN_IF(gs.alloc((size_t)D * esize(wdt)));
+  EDK_RETURN_IF(ss.alloc(sizeof(double)));
+  EDK_RETURN_IF(lanczos_common(op, opts, v0, v0_dtype, ptr_kind, evals, nullptr, nullptr, diag,
+                               gs.p));
+  std::lock_guard<std::mutex> lk(op->mu);
+  cudaStream_t st = op->stream;
+  const int64_t nd = D * (cx ? 2 : 1);  // real doubles
+  EDK_TRY_CUDA(cudaMemsetAsync(ss.p, 0, sizeof(double), st));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((nd + 255) / 256, 148 * 8));
+  gs_detail::k_sumsq<double><<<grid, 256, 0, st>>>(gs.as<double>(), nd, ss.as<double>());
+  gs_detail::k_scale_d<<<grid, 256, 0, st>>>(gs.as<double>(), nd, ss.as<double>());
+  EDK_TRY_CUDA(cudaGetLastError());
+  EDK_TRY_CUDA(cudaMemcpyAsync(psi, gs.p, (size_t)D * esize(wdt),
+                               ptr_kind == EDK_DEVICE ? cudaMemcpyDeviceToDevice
+                                                      : cudaMemcpyDeviceToHost, st));
+  EDK_TRY_CUDA(cudaStreamSynchronize(st));
+  return EDK_OK;
+}
+
+static edk_status lanczos_common(edk_operator* op, const edk_lanczos_opts* opts, const void* v0,
+                                 int32_t v0_dtype, int32_t ptr_kind, double* evals,
+                                 double* alpha, double* beta, edk_lanczos_diag* diag,
+                                 void* gs_out) {
   EDK_CHECK_ARG(op && opts && v0 && evals, "edk_lanczos_e0: NULL argument");
   EDK_CHECK_ARG(opts->max_steps >= 1, "edk_lanczos_e0: max_steps < 1");
   EDK_CHECK_ARG(opts->nev >= 1, "edk_lanczos_e0: nev < 1");
@@ -551,7 +620,7 @@ extern "C" edk_status edk_lanczos_e0(edk_operator* op, const edk_lanczos_opts* o
     o.max_steps = (int)std::min<int64_t>(o.max_steps, D);
     std::vector<OpResult> res;
     std::vector<edk_operator*> one(1, op);
-    EDK_RETURN_IF(batch_lanczos(one, o, src, v0_dtype, st, res, diag));
+    EDK_RETURN_IF(batch_lanczos(one, o, src, v0_dtype, st, res, diag, gs_out));
     const OpResult& r = res[0];
     for (int q = 0; q < opts->nev; ++q) evals[q] = q < (int)r.ev.size() ? r.ev[q] : NAN;
     if (alpha) for (int q = 0; q < r.steps; ++q) alpha[q] = r.a[q];
@@ -606,11 +675,13 @@ extern "C" edk_status edk_lanczos_e0(edk_operator* op, const edk_lanczos_opts* o
       R = R2;
       if (done || change <= tol) {
         bd = R2.breakdown;
+        if (gs_out) EDK_RETURN_IF(ritz_vector(F, R2, gs_out));
         break;
       }
       EDK_RETURN_IF(ritz_vector(F, R2, y.p));
     }
   }
+  if (!mixed && gs_out) EDK_RETURN_IF(ritz_vector(E, R, gs_out));
   for (int q = 0; q < opts->nev; ++q) evals[q] = q < (int)ev.size() ? ev[q] : NAN;
   if (alpha) for (int q = 0; q < R.steps; ++q) alpha[q] = R.a[q];
   if (beta) for (int q = 0; q < R.steps; ++q) beta[q] = R.b[q];

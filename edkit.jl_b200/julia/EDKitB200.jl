@@ -21,7 +21,7 @@ using EDKit, LinearAlgebra, SparseArrays
 import Base: *, size, eltype
 import LinearAlgebra: mul!
 
-export B200Operator, lanczos_e0, timeevolve, autotune!, block_lanczos
+export B200Operator, lanczos_e0, ground_state, timeevolve, autotune!, block_lanczos
 
 const libedk = get(ENV, "EDK_LIB", joinpath(@__DIR__, "..", "libedk.so"))
 
@@ -181,6 +181,27 @@ function lanczos_e0(H::B200Operator, v0::AbstractVector{T}; m::Integer=300, nev:
          Ptr{Float64}, Ref{LanczosDiag}), H.h, o, v, dtype_code(T), 0, ev, a, b, d))
     ev, d
 end
+
+"""
+    ground_state(H::B200Operator, v0; m=300, tol=1e-12, precision=:fp64) -> (E0, ψ, diag)
+
+E0 and the normalised lowest Ritz vector of the same Lanczos run.
+"""
+function ground_state(H::B200Operator, v0::AbstractVector{T}; m::Integer=300, tol::Real=1e-12,
+                      check_every::Integer=10, precision::Symbol=:fp64,
+                      refine_steps::Integer=20) where T
+    v = Vector{T}(v0)
+    o = LanczosOpts(m, 1, tol, check_every, precision === :mixed ? 1 : 0, refine_steps, 1, 0)
+    ev = zeros(1)
+    Tψ = (T <: Complex || eltype(H) <: Complex) ? ComplexF64 : Float64
+    ψ = zeros(Tψ, H.D)
+    d = LanczosDiag()
+    GC.@preserve v ev ψ check(ccall((:edk_lanczos_ground_state, libedk), Cint,
+        (Ptr{Cvoid}, Ref{LanczosOpts}, Ptr{T}, Int32, Int32, Ptr{Float64}, Ptr{Tψ}, Int32,
+         Ref{LanczosDiag}), H.h, o, v, dtype_code(T), 0, ev, ψ, dtype_code(Tψ), d))
+    ev[1], ψ, d
+end
+eltype(::B200Operator{Tv}) where Tv = Tv
 
 """
     timeevolve(H::B200Operator, ψ0, ts; tol=1e-10, m_init=30, m_max=60, ...)

@@ -299,6 +299,18 @@ edk_status edk_lanczos_e0(edk_operator* op, const edk_lanczos_opts* opts, const 
                           int32_t v0_dtype, int32_t ptr_kind, double* evals, double* alpha,
                           double* beta, edk_lanczos_diag* diag);
 
+/* The same Lanczos run returning the ground state as well: psi (host or
+ * device, per ptr_kind, D elements) receives the normalised lowest Ritz
+ * vector in the FP64 working dtype — EDK_F64 when the operator and v0 are
+ * real, EDK_C128 otherwise (psi_dtype must say which).  With precision mixed
+ * the vector comes from the FP64 refinement.  No single reference call: it
+ * is the eigenvector half of eigen(SymTridiagonal) on _lanczos_build!'s basis
+ * (TimeEvolution.jl:250-323). */
+edk_status edk_lanczos_ground_state(edk_operator* op, const edk_lanczos_opts* opts,
+                                   const void* v0, int32_t v0_dtype, int32_t ptr_kind,
+                                   double* evals, void* psi, int32_t psi_dtype,
+                                   edk_lanczos_diag* diag);
+
 /* Adaptive Krylov exp(-iHt) psi — timeevolve (TimeEvolution.jl:563-577)
  * with the cache/controller of TimeEvolution.jl:166-520.  psi0 and out are
  * complex (EDK_C128 interleaved; out is N x nts column-major).  ts may be

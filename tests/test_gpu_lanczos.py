@@ -196,3 +196,26 @@ def test_timeevolve_mixed_precision_fidelity(ek):
     for i in range(len(ts)):
         fid = abs(np.vdot(a[:, i], m[:, i])) ** 2
         assert 1 - fid < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ground_state_vector(ek, O, precision):
+    """The returned ground state is normalised, satisfies H psi = E0 psi to the
+    residual the eigenvalue allows, and matches the dense eigenvector up to a
+    phase — on the batched path (translation sector, complex and real), the
+    dedicated-basis path and the generic path (AbelianBasis)."""
+    L = 14
+    cases = [
+        ek.trans_inv_operator(xxz(ek.spin, 1.0), 2, ek.TranslationalBasis(L=L, N=7, k=0)),
+        ek.trans_inv_operator(xxz(ek.spin, 1.0), 2, ek.TranslationalBasis(L=L, N=7, k=3)),
+        ek.trans_inv_operator(xxz(ek.spin, 1.0), 2, ek.basis(L=L, N=7, k=0, p=1)),
+    ]
+    for H in cases:
+        e0, psi, info = ek.ground_state(H, m=200, tol=1e-13, precision=precision)
+        assert abs(np.linalg.norm(psi) - 1) < 1e-12
+        r = H * psi - e0 * psi
+        assert np.linalg.norm(r) < 1e-6
+        M = H.todense()
+        w, Vd = np.linalg.eigh(M)
+        assert abs(e0 - w[0]) < 1e-10 * abs(w[0])
+        assert abs(abs(np.vdot(Vd[:, 0], psi)) - 1) < 1e-9
