@@ -778,26 +778,34 @@ edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczo
   int wdt = cx ? EDK_C128 : EDK_F64;
   // common lookup kind: translation sectors with and without phases share BK_TRANS
   int bk = ops[0]->b->dev.bk;
+  bool all_mat = true;  // materialised operators run on the sliced-ELL kernel, whatever the basis
+  for (auto* op : ops) all_mat = all_mat && op->sell_ok;
   bool ff = true;
   int64_t Dmin = INT64_MAX;
   for (auto* op : ops) {
     int k = op->b->dev.bk;
     if (k != bk) {
       if ((k == BK_TRANS0 || k == BK_TRANS) && (bk == BK_TRANS0 || bk == BK_TRANS)) bk = BK_TRANS;
-      else { set_error("batch Lanczos: operators of different basis kinds"); return EDK_UNSUPPORTED; }
+      else if (!all_mat) {
+        set_error("batch Lanczos: operators of different basis kinds");
+        return EDK_UNSUPPORTED;
+      }
     }
     ff = ff && op->ff_ok && op->use_ff;
     if (!op->gather) {
       set_error("batch Lanczos: an operator is not Hermitian in its basis");
       return EDK_NOT_HERMITIAN;
     }
-    if (op->b->L > 32) {
-      set_error("batch Lanczos: L > 32 is not supported");
+    if (op->b->L > 32 && !op->sell_ok) {
+      set_error("batch Lanczos: L > 32 runs only on materialised operators");
       return EDK_UNSUPPORTED;
     }
     Dmin = std::min<int64_t>(Dmin, op->b->D);
   }
-  if (bk == BK_ABELIAN) { set_error("batch Lanczos: abelian bases run one at a time"); return EDK_UNSUPPORTED; }
+  if (bk == BK_ABELIAN && !all_mat) {
+    set_error("batch Lanczos: symmetry-group (abelian) bases run one at a time unless materialised");
+    return EDK_UNSUPPORTED;
+  }
   (void)Dmin;  // operators smaller than max_steps stop by the breakdown rule
   BatchEngine E;
   double ts0 = wall();

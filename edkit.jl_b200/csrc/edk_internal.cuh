@@ -226,6 +226,8 @@ struct SellDev {
   const int* width;        // entries per lane of each slice
   const int* col;          // target rows
   const uint16_t* code;    // coefficient codes
+  const double2* val;      // value mode (any operator): the entry's coefficient c, y += conj(c) x;
+                           // col holds the row, no codes (null in code mode)
   const double* diag;      // real diagonal per slot (Hermitian operators with real terms)
   const double2* diagc;    // complex diagonal per slot, or null
   const double* rinv;      // 1 / R of each norm class (1 for bases without norms)
@@ -273,7 +275,7 @@ struct edk_operator {
   edk::DevBuf fam, term, colptr, xmask, val, dval;
   edk::DevBuf hx, hy;  // staging buffers of edk_apply's host-pointer path (grow only)
   // materialised matrix (edk_operator_materialize)
-  edk::DevBuf s_rowid, s_off, s_width, s_col, s_code, s_diag, s_vt64, s_vt32, s_rinv, s_err;
+  edk::DevBuf s_rowid, s_off, s_width, s_col, s_code, s_diag, s_vt64, s_vt32, s_rinv, s_err, s_val;
   int64_t sell_wincap = 0;  // entries of the largest 256-row window
   bool sell_tma_ok = false;  // the staged (bulk-copy) product applies (stages fit in shared memory)
   bool sell_tma = false;     // ... and is used (set by the autotuner)

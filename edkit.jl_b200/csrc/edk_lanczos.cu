@@ -606,7 +606,7 @@ static edk_status lanczos_common(edk_operator* op, const edk_lanczos_opts* opts,
   cudaStream_t st = op->stream;
   const int64_t D = op->b->D;
   EDK_CHECK_ARG(D >= 1, "edk_lanczos_e0: empty basis");
-  if (op->b->L <= 32 && op->b->dev.bk != BK_ABELIAN && opts->reorth) {
+  if (((op->b->L <= 32 && op->b->dev.bk != BK_ABELIAN) || op->sell_ok) && opts->reorth) {
     // batch of one: device-side recurrence, graph-replayed steps
     DevBuf v0d;
     size_t es = (v0_dtype == EDK_F64 || v0_dtype == EDK_C64) ? 8 : (v0_dtype == EDK_C128 ? 16 : 4);

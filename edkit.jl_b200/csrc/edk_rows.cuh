@@ -422,7 +422,27 @@ __device__ __forceinline__ void sell_slice(const BasisDev& b, const SellDev& sd,
     }
   };
   int k = 0;
-  if (PACKED == 1 || (PACKED < 0 && sd.packed)) {
+  if (PACKED == 2 || (PACKED < 0 && sd.val)) {  // value mode: explicit coefficients
+    const int* cp = sd.col + base;
+    const double2* vp = sd.val + base;
+    auto vterm = [&](int c, double2 v) {
+      const Cx<A> xv = ldv(xk + c);
+      const A vr = (A)v.x, vi = (A)v.y;
+      if constexpr (CX) {
+        ar += vr * xv.r + vi * xv.i;  // conj(v) * x
+        ai += vr * xv.i - vi * xv.r;
+      } else {
+        ar += vr * xv.r;
+      }
+    };
+    for (; k + 2 <= w; k += 2) {
+      const int c0 = __ldcs(cp + (k + 0) * 32), c1 = __ldcs(cp + (k + 1) * 32);
+      const double2 v0 = __ldcs(vp + (k + 0) * 32), v1 = __ldcs(vp + (k + 1) * 32);
+      vterm(c0, v0);
+      vterm(c1, v1);
+    }
+    for (; k < w; ++k) vterm(__ldcs(cp + k * 32), __ldcs(vp + k * 32));
+  } else if (PACKED == 1 || (PACKED < 0 && sd.packed)) {
     const unsigned* ep = reinterpret_cast<const unsigned*>(sd.col + base);
     const int sh = sd.packed;
     const unsigned cm = (1u << sh) - 1u;

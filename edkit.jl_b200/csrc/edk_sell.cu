@@ -313,6 +313,76 @@ __global__ void __launch_bounds__(256) k_sell_tma(BasisDev b, SellDev sd,
   }
 }
 
+// Value mode (any operator in the row-gather form, any basis): the row
+// expansion of the generic kernel, stored with explicit coefficients
+// c = v * phase * R[target] / R[row], y_row += conj(c) x[target].
+template <int BK, class S>
+__global__ void __launch_bounds__(256) k_vsell_count(BasisDev b, OpDev op, int* __restrict__ cnt,
+                                                     double2* __restrict__ diag) {
+  __shared__ uint32_t s_binom[(BK == BK_PROJ_RANK) ? 32 * 33 : 1];
+  if constexpr (BK == BK_PROJ_RANK) {
+    fill_binom32(s_binom);
+    __syncthreads();
+  }
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < b.D;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const S s = (BK == BK_TENSOR) ? (S)i : (S)__ldg(b.I + i);
+    double dr = 0.0, di = 0.0;
+    int n = 0;
+    expand_row<BK, S>(b, op, s, s_binom, dr, di, [&](const Hit&, double, double) { ++n; });
+    cnt[i] = n;
+    diag[i] = make_double2(dr, di);
+  }
+}
+
+template <int BK, class S>
+__global__ void __launch_bounds__(256) k_vsell_fill(BasisDev b, OpDev op, int64_t nslices,
+                                                    const int* __restrict__ rowid,
+                                                    const int64_t* __restrict__ off,
+                                                    const int* __restrict__ width,
+                                                    const double2* __restrict__ drows,
+                                                    double* __restrict__ diag,
+                                                    double2* __restrict__ diagc,
+                                                    int* __restrict__ col,
+                                                    double2* __restrict__ val) {
+  __shared__ uint32_t s_binom[(BK == BK_PROJ_RANK) ? 32 * 33 : 1];
+  if constexpr (BK == BK_PROJ_RANK) {
+    fill_binom32(s_binom);
+    __syncthreads();
+  }
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < nslices * 32;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t slice = g >> 5;
+    const int row = rowid[g];
+    const int w = width[slice];
+    const int64_t base = off[slice] + (g & 31);
+    int k = 0;
+    if (row >= 0) {
+      const S s = (BK == BK_TENSOR) ? (S)row : (S)__ldg(b.I + row);
+      const double invRi = b.R ? 1.0 / __ldg(b.R + row) : 1.0;
+      double dr = 0.0, di = 0.0;
+      expand_row<BK, S>(b, op, s, s_binom, dr, di, [&](const Hit& h, double vr, double vi) {
+        if (k >= w) return;
+        const double ratio = h.rpos * invRi;
+        col[base + (int64_t)k * 32] = (int)h.pos;
+        val[base + (int64_t)k * 32] = make_double2((vr * h.pre - vi * h.pim) * ratio,
+                                                   (vr * h.pim + vi * h.pre) * ratio);
+        ++k;
+      });
+      const double2 d = drows[row];
+      if (diagc) diagc[g] = d;
+      else diag[g] = d.x;
+    } else {
+      if (diagc) diagc[g] = make_double2(0.0, 0.0);
+      else diag[g] = 0.0;
+    }
+    for (; k < w; ++k) {  // padding: coefficient 0 on a valid row
+      col[base + (int64_t)k * 32] = row >= 0 ? row : 0;
+      val[base + (int64_t)k * 32] = make_double2(0.0, 0.0);
+    }
+  }
+}
+
 int gridn(int64_t n) {
   int64_t g = (n + 255) / 256;
   return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
@@ -365,7 +435,9 @@ static edk_status launch_sell(const BasisDev& b, const SellDev& sd, const void* 
     dim3 grid((unsigned)((sd.nslices + 7) / 8), (unsigned)nk);
     const VT* xs = static_cast<const VT*>(x) + k0 * ldx;
     VT* ys = static_cast<VT*>(y) + k0 * ldy;
-    if (sd.packed)
+    if (sd.val)
+      k_sell_apply<VT, 2><<<grid, 256, 0, st>>>(b, sd, xs, ys, ldx, ldy, accumulate, 0);
+    else if (sd.packed)
       k_sell_apply<VT, 1><<<grid, 256, 0, st>>>(b, sd, xs, ys, ldx, ldy, accumulate, 0);
     else
       k_sell_apply<VT, 0><<<grid, 256, 0, st>>>(b, sd, xs, ys, ldx, ldy, accumulate, 0);
@@ -384,7 +456,9 @@ static edk_status launch_sell_rows(const BasisDev& b, const SellDev& sd, const v
   const VT* xs = static_cast<const VT*>(x);
   VT* ys = static_cast<VT*>(y);
   const int64_t D = b.D;
-  if (sd.packed)
+  if (sd.val)
+    k_sell_apply<VT, 2><<<(unsigned)(w1 - w0), 256, 0, st>>>(b, sd, xs, ys, D, D, accumulate, w0);
+  else if (sd.packed)
     k_sell_apply<VT, 1><<<(unsigned)(w1 - w0), 256, 0, st>>>(b, sd, xs, ys, D, D, accumulate, w0);
   else
     k_sell_apply<VT, 0><<<(unsigned)(w1 - w0), 256, 0, st>>>(b, sd, xs, ys, D, D, accumulate, w0);
@@ -444,31 +518,29 @@ edk_status apply_sell(edk_operator* op, int dtype, const void* x, void* y, int64
   return EDK_INVALID_ARG;
 }
 
+static edk_status materialize_values(edk_operator* op);
+
 static edk_status materialize(edk_operator* op) {
   edk_basis* bb = op->b;
   const BasisDev& b = bb->dev;
   const int bk = b.bk;
-  if (!(op->ff_ok && op->gather && bb->L <= 32 &&
-        (bk == BK_TENSOR || bk == BK_PROJ_RANK || bk == BK_PROJ_HASH || bk == BK_TRANS0 ||
-         bk == BK_TRANS || bk == BK_TRANSPAR))) {
-    set_error("edk_operator_materialize: only Hermitian operators of XXZ-type bond families "
-              "(plus diagonal terms) on spin-1/2 bases with L <= 32 are materialised");
+  if (!op->gather) {
+    set_error("edk_operator_materialize: the operator is not Hermitian (or not symmetric) in "
+              "this basis; only the row-gather form is materialised");
     return EDK_UNSUPPORTED;
   }
+  const bool coded = op->ff_ok && bb->L <= 32 &&
+                     (bk == BK_TENSOR || bk == BK_PROJ_RANK || bk == BK_PROJ_HASH ||
+                      bk == BK_TRANS0 || bk == BK_TRANS || bk == BK_TRANSPAR);
   const bool symm = bk == BK_TRANS0 || bk == BK_TRANS || bk == BK_TRANSPAR;
-  if (symm && !b.packed) {
-    set_error("edk_operator_materialize: too many distinct orbit norms for coefficient codes");
-    return EDK_UNSUPPORTED;
-  }
+  // bond-family operators: coefficient codes; everything else: explicit values
+  if (!coded || (symm && !b.packed)) return materialize_values(op);
   const FFParams& ff = *reinterpret_cast<const FFParams*>(op->ff_params.data());
   const int nval = 2 * ff.nfam;
   const int nph = (bk == BK_TRANS) ? b.len : (bk == BK_TRANSPAR ? 2 : 1);
   const int ncls = symm ? std::max(1, b.nclass) : 1;
   const int64_t ncode = 1 + (int64_t)nval * nph * ncls;
-  if (ncode > 65535) {
-    set_error("edk_operator_materialize: more than 65535 distinct coefficients");
-    return EDK_UNSUPPORTED;
-  }
+  if (ncode > 65535) return materialize_values(op);
   cudaStream_t st = op->stream;
   const int64_t D = b.D;
   // slot word row | class << rbits: 27 row bits under translations (<= 32
@@ -591,7 +663,9 @@ static edk_status materialize(edk_operator* op) {
   EDK_TRY_CUDA(cudaMemcpyAsync(op->s_vt32.p, vt32.data(), vt32.size() * sizeof(float2),
                                cudaMemcpyHostToDevice, st));
   EDK_TRY_CUDA(cudaStreamSynchronize(st));
+  op->s_val.release();
   SellDev& sd = op->dev.sell;
+  sd = SellDev{};
   sd.nslices = nslices;
   sd.packed = packed;
   sd.rbits = rbits;
@@ -627,6 +701,149 @@ static edk_status materialize(edk_operator* op) {
 
 using namespace edk;
 
+namespace edk {
+// Explicit-value sliced ELL for any operator in the row-gather form.
+static edk_status materialize_values(edk_operator* op) {
+  edk_basis* bb = op->b;
+  const BasisDev& b = bb->dev;
+  const int bk = b.bk;
+  cudaStream_t st = op->stream;
+  const int64_t D = b.D;
+  if (D >= (int64_t(1) << 31)) {
+    set_error("edk_operator_materialize: basis dimension too large for the sliced-ELL row index");
+    return EDK_UNSUPPORTED;
+  }
+  EDK_RETURN_IF(check_basis_dev(b));
+  const bool wide = bb->L > 32;
+  DevBuf cnt, drows;
+  EDK_RETURN_IF(cnt.alloc(std::max<int64_t>(D, 1) * sizeof(int)));
+  EDK_RETURN_IF(drows.alloc(std::max<int64_t>(D, 1) * sizeof(double2)));
+#define EDK_VCNT(BK)                                                                            \
+  case BK:                                                                                      \
+    if (wide) k_vsell_count<BK, uint64_t><<<gridn(D), 256, 0, st>>>(b, op->dev, cnt.as<int>(),  \
+                                                                   drows.as<double2>());       \
+    else k_vsell_count<BK, uint32_t><<<gridn(D), 256, 0, st>>>(b, op->dev, cnt.as<int>(),       \
+                                                              drows.as<double2>());            \
+    break;
+  switch (bk) {
+    EDK_VCNT(BK_TENSOR)
+    EDK_VCNT(BK_PROJ_RANK)
+    EDK_VCNT(BK_PROJ_HASH)
+    EDK_VCNT(BK_TRANS0)
+    EDK_VCNT(BK_TRANS)
+    EDK_VCNT(BK_TRANSPAR)
+    EDK_VCNT(BK_ABELIAN)
+    default:
+      set_error("edk_operator_materialize: unknown lookup kind");
+      return EDK_INVALID_ARG;
+  }
+#undef EDK_VCNT
+  EDK_TRY_CUDA(cudaGetLastError());
+  std::vector<int> hc(D);
+  if (D > 0) EDK_TRY_CUDA(cudaMemcpyAsync(hc.data(), cnt.p, D * sizeof(int), cudaMemcpyDeviceToHost, st));
+  EDK_TRY_CUDA(cudaStreamSynchronize(st));
+  const int64_t nwin = (D + 255) / 256;
+  const int64_t nslices = nwin * 8;
+  std::vector<int> rowid((size_t)nslices * 32, -1), width(nslices, 0);
+  std::vector<int64_t> off(nslices, 0);
+  int64_t E = 0;
+  std::vector<int> order;
+  for (int64_t wdx = 0; wdx < nwin; ++wdx) {
+    const int64_t r0 = wdx * 256, r1 = std::min<int64_t>(D, r0 + 256);
+    order.clear();
+    for (int64_t r = r0; r < r1; ++r) order.push_back((int)r);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return hc[a] > hc[c]; });
+    for (size_t q = 0; q < order.size(); ++q) rowid[(size_t)wdx * 256 + q] = order[q];
+    for (int sl = 0; sl < 8; ++sl) {
+      const int64_t s = wdx * 8 + sl;
+      const int first = rowid[(size_t)s * 32];
+      width[s] = first >= 0 ? hc[first] : 0;
+      off[s] = E;
+      E += (int64_t)width[s] * 32;
+    }
+  }
+  if (E >= (int64_t(1) << 40)) {
+    set_error("edk_operator_materialize: too many entries");
+    return EDK_UNSUPPORTED;
+  }
+  EDK_RETURN_IF(op->s_rowid.alloc(rowid.size() * sizeof(int)));
+  EDK_RETURN_IF(op->s_width.alloc(width.size() * sizeof(int)));
+  EDK_RETURN_IF(op->s_off.alloc(off.size() * sizeof(int64_t)));
+  EDK_RETURN_IF(op->s_col.alloc(std::max<int64_t>(E, 1) * sizeof(int)));
+  EDK_RETURN_IF(op->s_val.alloc(std::max<int64_t>(E, 1) * sizeof(double2)));
+  op->s_code.release();
+  const bool dcx = op->is_complex;
+  EDK_RETURN_IF(op->s_diag.alloc(nslices * 32 * (dcx ? sizeof(double2) : sizeof(double))));
+  double* dre = dcx ? nullptr : op->s_diag.as<double>();
+  double2* dcp = dcx ? op->s_diag.as<double2>() : nullptr;
+  EDK_TRY_CUDA(cudaMemcpyAsync(op->s_rowid.p, rowid.data(), rowid.size() * sizeof(int),
+                               cudaMemcpyHostToDevice, st));
+  EDK_TRY_CUDA(cudaMemcpyAsync(op->s_width.p, width.data(), width.size() * sizeof(int),
+                               cudaMemcpyHostToDevice, st));
+  EDK_TRY_CUDA(cudaMemcpyAsync(op->s_off.p, off.data(), off.size() * sizeof(int64_t),
+                               cudaMemcpyHostToDevice, st));
+#define EDK_VFILL(BK)                                                                           \
+  case BK:                                                                                      \
+    if (wide)                                                                                   \
+      k_vsell_fill<BK, uint64_t><<<gridn(nslices * 32), 256, 0, st>>>(                          \
+          b, op->dev, nslices, op->s_rowid.as<int>(), op->s_off.as<int64_t>(),                 \
+          op->s_width.as<int>(), drows.as<double2>(), dre, dcp, op->s_col.as<int>(),           \
+          op->s_val.as<double2>());                                                            \
+    else                                                                                        \
+      k_vsell_fill<BK, uint32_t><<<gridn(nslices * 32), 256, 0, st>>>(                          \
+          b, op->dev, nslices, op->s_rowid.as<int>(), op->s_off.as<int64_t>(),                 \
+          op->s_width.as<int>(), drows.as<double2>(), dre, dcp, op->s_col.as<int>(),           \
+          op->s_val.as<double2>());                                                            \
+    break;
+  switch (bk) {
+    EDK_VFILL(BK_TENSOR)
+    EDK_VFILL(BK_PROJ_RANK)
+    EDK_VFILL(BK_PROJ_HASH)
+    EDK_VFILL(BK_TRANS0)
+    EDK_VFILL(BK_TRANS)
+    EDK_VFILL(BK_TRANSPAR)
+    EDK_VFILL(BK_ABELIAN)
+  }
+#undef EDK_VFILL
+  EDK_TRY_CUDA(cudaGetLastError());
+  std::vector<double> rinv(32, 1.0);
+  EDK_RETURN_IF(op->s_rinv.alloc(rinv.size() * sizeof(double)));
+  EDK_TRY_CUDA(cudaMemcpyAsync(op->s_rinv.p, rinv.data(), rinv.size() * sizeof(double),
+                               cudaMemcpyHostToDevice, st));
+  std::vector<double2> vt(1, make_double2(0.0, 0.0));
+  std::vector<float2> vt32(1, make_float2(0.f, 0.f));
+  EDK_RETURN_IF(op->s_vt64.alloc(sizeof(double2)));
+  EDK_RETURN_IF(op->s_vt32.alloc(sizeof(float2)));
+  EDK_TRY_CUDA(cudaMemcpyAsync(op->s_vt64.p, vt.data(), sizeof(double2), cudaMemcpyHostToDevice, st));
+  EDK_TRY_CUDA(cudaMemcpyAsync(op->s_vt32.p, vt32.data(), sizeof(float2), cudaMemcpyHostToDevice, st));
+  EDK_RETURN_IF(op->s_err.alloc(sizeof(int)));
+  EDK_TRY_CUDA(cudaMemsetAsync(op->s_err.p, 0, sizeof(int), st));
+  EDK_TRY_CUDA(cudaStreamSynchronize(st));
+  SellDev& sd = op->dev.sell;
+  sd = SellDev{};
+  sd.nslices = nslices;
+  sd.packed = 0;
+  sd.rbits = 31;
+  sd.rowid = op->s_rowid.as<unsigned>();
+  sd.off = op->s_off.as<int64_t>();
+  sd.width = op->s_width.as<int>();
+  sd.col = op->s_col.as<int>();
+  sd.code = nullptr;
+  sd.val = op->s_val.as<double2>();
+  sd.diag = dre;
+  sd.diagc = dcp;
+  sd.rinv = op->s_rinv.as<double>();
+  sd.vt64 = op->s_vt64.as<double2>();
+  sd.vt32 = op->s_vt32.as<float2>();
+  op->sell_wincap = 0;
+  op->sell_tma_ok = false;
+  op->sell_tma = false;
+  op->sell_entries = E;
+  op->sell_ok = true;
+  return EDK_OK;
+}
+}  // namespace edk
+
 extern "C" edk_status edk_operator_materialize(edk_operator* op, int32_t enable,
                                                int64_t* entries) {
   EDK_CHECK_ARG(op != nullptr, "edk_operator_materialize: NULL operator");
@@ -636,7 +853,7 @@ extern "C" edk_status edk_operator_materialize(edk_operator* op, int32_t enable,
     op->dev.sell = SellDev{};
     op->s_rowid.release(); op->s_off.release(); op->s_width.release(); op->s_col.release();
     op->s_code.release(); op->s_diag.release(); op->s_vt64.release(); op->s_vt32.release();
-    op->s_rinv.release();
+    op->s_rinv.release(); op->s_val.release();
     op->sell_entries = 0;
     if (entries) *entries = 0;
     return EDK_OK;

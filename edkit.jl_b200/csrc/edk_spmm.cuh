@@ -201,7 +201,12 @@ __global__ void __launch_bounds__(256) k_spmm_sell(const SpmmOp* __restrict__ op
       const int k = kb + lane;
       int col = 0;
       double cr = 0.0, ci = 0.0;
-      if (k < w) {
+      if (k < w && sd.val) {  // value mode: explicit coefficients, already divided by R[row]
+        col = __ldg(sd.col + base + (int64_t)k * 32);
+        const double2 v = __ldg(sd.val + base + (int64_t)k * 32);
+        cr = v.x;
+        ci = v.y;
+      } else if (k < w) {
         int code;
         if (sd.packed) {
           const unsigned e =

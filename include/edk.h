@@ -164,12 +164,16 @@ edk_status edk_operator_info(const edk_operator* op, int32_t* gather, int32_t* i
                              int32_t* n_families, int32_t* n_generic);
 
 /* sparse!(opt) / clear_sparse_cache! (Operator.jl:221-285) for the device:
- * enable=1 expands every row once into a cached sliced-ELLPACK matrix (4-byte
- * target row + 2-byte coefficient code per nonzero) that every later
- * edk_apply / edk_lanczos_e0 / edk_krylov_evolve / batch call on this operator
- * uses; enable=0 frees it.  *entries (may be NULL) receives the number of
- * stored entries.  Available for Hermitian operators built from XXZ-type bond
- * families plus diagonal terms on spin-1/2 bases with L <= 32. */
+ * enable=1 expands every row once into a cached sliced-ELLPACK matrix that
+ * every later edk_apply / edk_lanczos_e0 / edk_krylov_evolve / batch call on
+ * this operator uses; enable=0 frees it.  *entries (may be NULL) receives the
+ * number of stored entries.  Bond-family operators (XXZ-type bonds plus
+ * diagonal terms, L <= 32) store a target row and a coefficient code per
+ * nonzero (4 bytes when they fit one word); every other operator in the
+ * row-gather form (Hermitian and symmetric under its basis: generic terms,
+ * symmetry-group and dedicated bases, L up to 63) stores the row and the
+ * explicit complex coefficient (20 bytes).  Materialised operators of any
+ * basis kind run batched. */
 edk_status edk_operator_materialize(edk_operator* op, int32_t enable, int64_t* entries);
 
 /* Block Lanczos over a batch of operators (e.g. the momentum sectors of one
