@@ -827,8 +827,17 @@ edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczo
   EDK_RETURN_IF(E.capture());
   EDK_TRY_CUDA(cudaStreamSynchronize(st));
   double ts1 = wall();
-  double tol1 = mixed ? std::max(o.tol, 1e-7) : o.tol;
-  EDK_RETURN_IF(run_batch(E, o.max_steps, o.nev, tol1, o.check_every, res, &nchecks));
+  // mixed stage 1 (FP32 vectors): its Ritz values move by rounding at ~1e-7,
+  // so it stops well above that — a ground state needs only a good start for
+  // the FP64 refinement (1e-5), several levels a better one (1e-7) — and, for
+  // a few operators, it checks every 5 steps so that it stops early
+  double tol1 = mixed ? std::max(o.tol, o.nev > 1 ? 1e-7 : 1e-5) : o.tol;
+  // (a check solves every operator's tridiagonal problem on the host, so
+  // large batches keep the caller's interval)
+  const int check1 = (mixed && nops <= 8)
+                         ? std::max(1, std::min(o.check_every > 0 ? o.check_every : 5, 5))
+                         : o.check_every;
+  EDK_RETURN_IF(run_batch(E, o.max_steps, o.nev, tol1, check1, res, &nchecks));
   double ts2 = wall();
   int rounds = 0;
   for (int q = 0; q < nops; ++q)
@@ -843,13 +852,12 @@ edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczo
   for (int q = 0; q < nops; ++q) goff[q] = E.hops[q].woff;
   if (!mixed && ritz_out) EDK_RETURN_IF(ritz_vectors(E, res, ritz_out, 1));
   if (mixed) {
-    // FP64 refinement restarted from the sum of the nev lowest Ritz vectors.
-    // A single eigenvalue converges in a few steps from its FP32 Ritz vector;
-    // several need room to separate close levels, so the round may run to
-    // max_steps (each operator stops when it converges).  Operators that
-    // reach the step limit without converging are restarted again, alone.
-    const int mr = o.nev > 1 ? std::max(o.max_steps, o.refine_steps)
-                             : (o.refine_steps > 0 ? o.refine_steps : 20);
+    // FP64 refinement restarted from the sum of the nev lowest Ritz vectors,
+    // in one round that may run to max_steps (each operator stops when it
+    // converges: a few steps for a ground state, more to separate close
+    // levels).  Operators that reach the step limit unconverged are
+    // restarted again, alone.
+    const int mr = std::max(o.max_steps, o.refine_steps);
     std::vector<int> active(nops);
     for (int q = 0; q < nops; ++q) active[q] = q;
     DevBuf cur;  // start vectors of `active`, compact in that order

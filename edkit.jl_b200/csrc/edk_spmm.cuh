@@ -69,6 +69,55 @@ __device__ __forceinline__ void store_row(VT* __restrict__ yr, int lane, int p, 
   }
 }
 
+// Apply the nh hits held one per lane (ok, target row, coefficient) to the
+// lane's columns, four hits at a time: their row gathers are all issued
+// before the multiply-adds, so four rows are in flight per lane.
+template <class VT, int VPL>
+__device__ __forceinline__ void apply_hits(typename VTraits<VT>::A (&ar)[VPL],
+                                           typename VTraits<VT>::A (&ai)[VPL],
+                                           const VT* __restrict__ xb, int lane, int p, int nh,
+                                           int ok, int64_t pos, double cr, double ci) {
+  using A = typename VTraits<VT>::A;
+  constexpr bool CX = VTraits<VT>::cx;
+  const unsigned full = 0xffffffffu;
+  int hh = 0;
+  for (; hh + 4 <= nh; hh += 4) {
+    int okq[4];
+    int64_t pq[4];
+    double crq[4], ciq[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      okq[u] = __shfl_sync(full, ok, hh + u);
+      pq[u] = __shfl_sync(full, pos, hh + u);
+      crq[u] = __shfl_sync(full, cr, hh + u);
+      ciq[u] = __shfl_sync(full, ci, hh + u);
+    }
+    Cx<A> xv[4][VPL];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        const int c = lane + 32 * v;
+        xv[u][v] = (okq[u] && c < p) ? ldv(xb + pq[u] * p + c) : Cx<A>{0, 0};
+      }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const A r = (A)crq[u], im = (A)ciq[u];
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        ar[v] += r * xv[u][v].r + im * xv[u][v].i;  // conj(coefficient) * x
+        if constexpr (CX) ai[v] += r * xv[u][v].i - im * xv[u][v].r;
+      }
+    }
+  }
+  for (; hh < nh; ++hh) {
+    if (!__shfl_sync(full, ok, hh)) continue;
+    const int64_t ph = __shfl_sync(full, pos, hh);
+    const double crh = __shfl_sync(full, cr, hh), cih = __shfl_sync(full, ci, hh);
+    acc_row<VT, VPL>(ar, ai, xb + ph * p, lane, p, crh, cih);
+  }
+}
+
 }  // namespace spmm_detail
 
 template <int BK, class VT, int VPL>
@@ -155,12 +204,7 @@ __global__ void __launch_bounds__(256) k_spmm_ff(const SpmmOp* __restrict__ ops,
         }
       }
       const int nh = min(32, nhit - base);
-      for (int hh = 0; hh < nh; ++hh) {
-        if (!__shfl_sync(full, ok, hh)) continue;
-        const int64_t ph = __shfl_sync(full, pos, hh);
-        const double crh = __shfl_sync(full, cr, hh), cih = __shfl_sync(full, ci, hh);
-        spmm_detail::acc_row<VT, VPL>(ar, ai, xb + ph * p, lane, p, crh, cih);
-      }
+      spmm_detail::apply_hits<VT, VPL>(ar, ai, xb, lane, p, nh, ok, pos, cr, ci);
     }
     spmm_detail::store_row<VT, VPL>(Y + (int64_t)q * Dpad * p + i * p, lane, p, accumulate, ar,
                                     ai);
@@ -222,12 +266,8 @@ __global__ void __launch_bounds__(256) k_spmm_sell(const SpmmOp* __restrict__ op
         ci = v.y * invR;
       }
       const int nh = min(32, w - kb);
-      for (int hh = 0; hh < nh; ++hh) {
-        const int ch = __shfl_sync(full, col, hh);
-        const double crh = __shfl_sync(full, cr, hh), cih = __shfl_sync(full, ci, hh);
-        if (crh == 0.0 && cih == 0.0) continue;  // padding entry (code 0)
-        spmm_detail::acc_row<VT, VPL>(ar, ai, xb + (int64_t)ch * p, lane, p, crh, cih);
-      }
+      // padding entries carry a zero coefficient: applying them adds nothing
+      spmm_detail::apply_hits<VT, VPL>(ar, ai, xb, lane, p, nh, 1, (int64_t)col, cr, ci);
     }
     spmm_detail::store_row<VT, VPL>(Y + (int64_t)q * Dpad * p + row * p, lane, p, accumulate,
                                     ar, ai);
