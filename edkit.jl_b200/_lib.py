@@ -25,6 +25,7 @@ EXPORTS = [
     "edk_basis_index", "edk_basis_index_noalloc", "edk_operator_create", "edk_operator_destroy", "edk_operator_info",
     "edk_operator_materialize", "edk_operator_configure", "edk_operator_autotune",
     "edk_basis_set_search", "edk_basis_get_search", "edk_block_lanczos", "edk_lanczos_ground_state",
+    "edk_block_tridiag_lowest",
     "edk_block_lanczos_default_opts",
     "edk_apply", "edk_apply_async", "edk_lanczos_e0", "edk_krylov_default_opts",
     "edk_krylov_evolve", "edk_batch_lanczos_e0", "edk_tridiag_eigen", "edk_last_error",
@@ -150,6 +151,7 @@ def load():
         "edk_apply_async": (st, [vp, i32, vp, vp, i64, i64, i64, i32, vp]),
         "edk_lanczos_e0": (st, [vp, C.POINTER(LanczosOpts), vp, i32, i32, vp, vp, vp,
                                 C.POINTER(LanczosDiag)]),
+        "edk_block_tridiag_lowest": (st, [i32, i32, vp, vp, i32, vp]),
         "edk_lanczos_ground_state": (st, [vp, C.POINTER(LanczosOpts), vp, i32, i32, vp, vp, i32,
                                           C.POINTER(LanczosDiag)]),
         "edk_krylov_default_opts": (None, [C.POINTER(KrylovOpts)]),

@@ -786,6 +786,22 @@ static edk_status block_lanczos(int nops, edk_operator* const* ops,
 
 using namespace edk;
 
+extern "C" edk_status edk_block_tridiag_lowest(int32_t p, int32_t m, const double* A,
+                                              const double* B, int32_t nev, double* out) {
+  EDK_CHECK_ARG(p >= 1 && m >= 1 && nev >= 1 && A && out && (m == 1 || B),
+                "edk_block_tridiag_lowest: bad argument");
+  const size_t pp = (size_t)p * p;
+  std::vector<const double*> Ap(m), Bp(m, nullptr);
+  for (int j = 0; j < m; ++j) {
+    Ap[j] = A + 2 * pp * j;
+    if (j >= 1) Bp[j] = B + 2 * pp * (j - 1);
+  }
+  std::vector<double> res;
+  band_lowest(Ap, Bp, p, m, nev, res);
+  for (int k = 0; k < nev; ++k) out[k] = k < (int)res.size() ? res[k] : NAN;
+  return EDK_OK;
+}
+
 extern "C" void edk_block_lanczos_default_opts(edk_block_lanczos_opts* o) {
   if (!o) return;
   o->block = 64;

@@ -206,6 +206,15 @@ typedef struct {
   double seconds, seconds_spmm, seconds_orth, seconds_eig;
 } edk_block_lanczos_diag;
 void edk_block_lanczos_default_opts(edk_block_lanczos_opts* opts);
+
+/* The eigenvalue step of edk_block_lanczos on a block-tridiagonal matrix the
+ * caller holds (host only, no device work): A = m diagonal blocks (p x p,
+ * column-major complex, interleaved re/im, Hermitian), B = m-1 sub-diagonal
+ * blocks T(j+1, j).  out = the lowest nev distinct eigenvalues, copies that a
+ * block Lanczos run without full re-orthogonalisation creates removed by the
+ * block Cullum-Willoughby test (NaN where fewer exist). */
+edk_status edk_block_tridiag_lowest(int32_t p, int32_t m, const double* A, const double* B,
+                                    int32_t nev, double* out);
 edk_status edk_block_lanczos(int32_t nops, edk_operator* const* ops,
                              const edk_block_lanczos_opts* opts, const double* x0, double* evals,
                              edk_block_lanczos_diag* diag);
