@@ -11,6 +11,7 @@ from .algorithms import (KrylovEvolutionDiagnostics, batch_lanczos_e0, block_lan
 from .basis import (AbelianBasis, AbstractBasis, FlipBasis, ParityBasis, ParityFlipBasis,
                     ProjectedBasis, TensorBasis, TranslationalBasis, TranslationFlipBasis,
                     TranslationParityBasis, basis)
+from .entanglement import DoubleBasis, ent_S, ent_spec, entropy, schmidt, symmetrizer
 from .operator import Operator, mul, mul_, operator, spin, trans_inv_operator, σ
 
 __all__ = [
@@ -20,6 +21,7 @@ __all__ = [
     "Operator", "mul", "mul_", "lanczos_e0", "ground_state", "batch_lanczos_e0", "block_lanczos",
     "timeevolve",
     "tridiag_eigen", "gapratio", "meangapratio", "productstate", "KrylovEvolutionDiagnostics", "version",
+    "schmidt", "ent_spec", "entropy", "ent_S", "DoubleBasis", "symmetrizer",
 ]
 
 

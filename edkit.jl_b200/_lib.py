@@ -25,6 +25,7 @@ EXPORTS = [
     "edk_basis_index", "edk_basis_index_noalloc", "edk_operator_create", "edk_operator_destroy", "edk_operator_info",
     "edk_operator_materialize", "edk_operator_configure", "edk_operator_autotune",
     "edk_basis_set_search", "edk_basis_get_search", "edk_block_lanczos", "edk_lanczos_ground_state",
+    "edk_schmidt", "edk_ent_spec", "edk_ent_S", "edk_double_basis_apply", "edk_symmetrizer",
     "edk_block_tridiag_lowest",
     "edk_block_lanczos_default_opts",
     "edk_apply", "edk_apply_async", "edk_lanczos_e0", "edk_krylov_default_opts",
@@ -160,6 +161,11 @@ def load():
         "edk_batch_lanczos_e0": (st, [i32, vp, C.POINTER(LanczosOpts), vp, i32, vp,
                                       C.POINTER(LanczosDiag)]),
         "edk_tridiag_eigen": (C.c_int, [C.c_int, vp, vp, vp, vp]),
+        "edk_schmidt": (st, [vp, i32, vp, i32, vp, vp, i32, i32]),
+        "edk_ent_spec": (st, [vp, i32, vp, i32, vp, vp, C.POINTER(i64), i32]),
+        "edk_ent_S": (st, [vp, i32, vp, i32, vp, C.c_double, C.c_double, dp, i32]),
+        "edk_double_basis_apply": (st, [vp, vp, i32, vp, vp, i32]),
+        "edk_symmetrizer": (st, [vp, vp, vp, i32]),
         "edk_last_error": (C.c_char_p, []),
         "edk_version": (C.c_char_p, []),
     }

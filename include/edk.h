@@ -369,6 +369,50 @@ edk_status edk_batch_lanczos_e0(int32_t nops, edk_operator* const* ops,
  * eigenvectors column-major m x m.  Returns 0 on success. */
 int edk_tridiag_eigen(int m, const double* a, const double* b, double* w, double* Q);
 
+/*
+ * Eigenvector post-processing (base 2, L <= 32).
+ *
+ * schmidt(v, Ainds, b) — src/Schmidt.jl:186-336 (TensorBasis / ProjectedBasis,
+ * TranslationalBasis, TranslationParityBasis and TranslationFlipBasis through
+ * parity_schmidt, FlipBasis, ParityBasis, ParityFlipBasis) and
+ * src/Basis/AbelianBasis.jl:704-719 (AbelianBasis): the 2^nA x 2^(L-nA)
+ * Schmidt matrix of the sector vector v (length D, F64 or C128), column-major
+ * M[ia + ib * 2^nA].  Ainds: nA 1-based sites of subsystem A; row index =
+ * A digits big-endian in Ainds order, column index = the remaining sites
+ * ascending (schmidtmatrix, Schmidt.jl:39-57).  M is C128, or F64 when v is
+ * F64 and the basis phases are real.  ptr_kind applies to v and M.
+ */
+edk_status edk_schmidt(const edk_basis* b, int32_t vdtype, const void* v, int32_t nA,
+                       const int32_t* Ainds, void* M, int32_t mdtype, int32_t ptr_kind);
+/* ent_spec(v, Aind, b) — Schmidt.jl:84: singular values of the Schmidt matrix,
+ * descending, into s (host, min(2^nA, 2^(L-nA)) values, count in *ns; s may
+ * be NULL to query the count).  Computed as square roots of the eigenvalues
+ * of the Gram matrix of the smaller side (cuBLAS SYRK/HERK + cuSOLVER
+ * SYEVD/HEEVD); squared values below n * eps * max are returned as 0.
+ * min side <= 32768.  ptr_kind applies to v. */
+edk_status edk_ent_spec(const edk_basis* b, int32_t vdtype, const void* v, int32_t nA,
+                        const int32_t* Ainds, double* s, int64_t* ns, int32_t ptr_kind);
+/* ent_S(v, Aind, b; α, cutoff) — Schmidt.jl:101-153: entropy of the squared
+ * Schmidt values (α = 1: von Neumann with the cutoff break; α = 0: the count
+ * of values above the cutoff, as the reference returns it; otherwise Rényi
+ * log(Σ s^α) / (1 - α)). */
+edk_status edk_ent_S(const edk_basis* b, int32_t vdtype, const void* v, int32_t nA,
+                     const int32_t* Ainds, double alpha, double cutoff, double* S,
+                     int32_t ptr_kind);
+/* (B::DoubleBasis)(v) with B = DoubleBasis(B1, B2) — src/LinearMap.jl:140-166:
+ * out (C128, length D1) = Σ over full-space states of
+ * conj(c1 / order(B1)) * (c2 / order(B2)) * v[pos2], where (c, pos) = index().
+ * Both bases on one device with the same L and base
+ * (check_doublebasis_compatible, LinearMap.jl:38-42).  ptr_kind applies to v
+ * and out. */
+edk_status edk_double_basis_apply(const edk_basis* B1, const edk_basis* B2, int32_t vdtype,
+                                  const void* v, double* out, int32_t ptr_kind);
+/* symmetrizer(DoubleBasis(B1, B2)) — LinearMap.jl:183-185 with
+ * basis_embedding :57-70: the D1 x D2 C128 matrix
+ * basis_embedding(B1)' * basis_embedding(B2), column-major. */
+edk_status edk_symmetrizer(const edk_basis* B1, const edk_basis* B2, double* M,
+                           int32_t ptr_kind);
+
 /* last error message of the calling thread ("" if none) */
 const char* edk_last_error(void);
 /* library version string */

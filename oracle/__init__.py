@@ -241,14 +241,18 @@ def translational(L, k=0, N=None, a=1, f=None, base=2, threaded=True, gosper=Tru
     fn, keep = _pred(f)
     h = lib().orc_translational(L, base, k, -1 if N is None else N, a, fn, None,
                                 int(threaded), int(gosper))
-    return OBasis(h, L, base, keep)
+    ob = OBasis(h, L, base, keep)
+    ob.A = a
+    return ob
 
 
 def transparity(L, k=0, p=1, N=None, a=1, f=None, base=2, threaded=True, gosper=True):
     fn, keep = _pred(f)
     h = lib().orc_transparity(L, base, k, p, -1 if N is None else N, a, fn, None,
                               int(threaded), int(gosper))
-    return OBasis(h, L, base, keep)
+    ob = OBasis(h, L, base, keep)
+    ob.A, ob.P = a, p
+    return ob
 
 
 def abelian_generators(L, k=None, a=1, p=None, z=None, symmetries=None):
@@ -293,7 +297,9 @@ def abelian(L, N=None, k=None, a=1, p=None, z=None, symmetries=None, f=None, bas
     fn, keep = _pred(f)
     h = lib().orc_abelian(L, base, -1 if N is None else N, len(gens), _ptr(orders), _ptr(ks),
                           _ptr(perms), _ptr(invs), fn, None, int(threaded))
-    return OBasis(h, L, base, (keep, orders, ks, perms, invs))
+    ob = OBasis(h, L, base, (keep, orders, ks, perms, invs))
+    ob.gens = gens
+    return ob
 
 
 def basis(L, N=None, k=None, a=1, p=None, z=None, symmetries=None, f=None, base=2):
@@ -337,9 +343,12 @@ def _charge_ok(dgt, L, N, f):
 
 
 class DedicatedBasis:
-    def __init__(self, L, I, R, index_fn):
+    def __init__(self, L, I, R, index_fn, kind, **info):
         self.L, self.I, self.R, self._index = L, I, R, index_fn
         self.dim = len(I)
+        self.kind = kind  # "parity" | "flip" | "parityflip" | "transflip"
+        for k, v in info.items():
+            setattr(self, k, v)
 
     def index_state(self, s):
         return self._index(self, s)
@@ -367,7 +376,7 @@ def parity_basis(L, p, N=None, f=None):
         Ia, Ib = s + 1, _rev(s, L) + 1
         i, n = (_bsearch(b.I, Ib), p) if Ib < Ia else (_bsearch(b.I, Ia), 1)
         return (0.0, 1) if i == 0 else (n * b.R[i - 1], i)
-    return DedicatedBasis(L, I, R, index)
+    return DedicatedBasis(L, I, R, index, "parity", P=p)
 
 
 def flip_basis(L, p, N=None, f=None):
@@ -395,7 +404,7 @@ def flip_basis(L, p, N=None, f=None):
         Ib = MAX - Ia
         i, n = (_bsearch(b.I, Ib), p) if Ib < Ia else (_bsearch(b.I, Ia), 1)
         return (0.0, 1) if i == 0 else (n * b.R[i - 1], i)
-    return DedicatedBasis(L, I, R, index)
+    return DedicatedBasis(L, I, R, index, "flip", P=p)
 
 
 def parityflip_basis(L, p, z, N=None, f=None):
@@ -451,7 +460,7 @@ def parityflip_basis(L, p, z, N=None, f=None):
         if Ir == Iz:
             return (z * r, i)
         return (p * z * r, i)
-    return DedicatedBasis(L, I, R, index)
+    return DedicatedBasis(L, I, R, index, "parityflip", P=p, Z=z)
 
 
 def _phase_factor(k, length):  # TranslationalBasis.jl:277-285
@@ -532,7 +541,7 @@ def transflip_basis(L, k=0, p=1, N=None, a=1, f=None):
         else:
             i, n = _bsearch(b.I, Iam), Cph[Rm]
         return (0.0, 1) if i == 0 else (n * b.R[i - 1], i)
-    return DedicatedBasis(L, I, R, index)
+    return DedicatedBasis(L, I, R, index, "transflip", P=p, C=Cph, A=a)
 
 
 class OOperator:
