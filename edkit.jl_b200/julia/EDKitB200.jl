@@ -21,7 +21,8 @@ using EDKit, LinearAlgebra, SparseArrays
 import Base: *, size, eltype
 import LinearAlgebra: mul!
 
-export B200Operator, lanczos_e0, ground_state, timeevolve, autotune!, block_lanczos
+export B200Operator, B200Basis, lanczos_e0, ground_state, timeevolve, autotune!, block_lanczos,
+       schmidt_b200, ent_S_b200, double_basis_b200, symmetrizer_b200
 
 const libedk = get(ENV, "EDK_LIB", joinpath(@__DIR__, "..", "libedk.so"))
 
@@ -288,5 +289,69 @@ end
 timeevolve(H::B200Operator, ψ0::AbstractVector, t::Real; kw...) =
     (t < 0 && error("timeevolve!: requested time $t precedes anchor time 0.0");
      timeevolve(H, ψ0, [t]; kw...)[:, 1])
+
+# --- eigenvector post-processing (src/Schmidt.jl, src/LinearMap.jl) ---
+_vdt(::AbstractVector{Float64}) = Int32(0)
+_vdt(::AbstractVector{ComplexF64}) = Int32(1)
+
+"""
+    schmidt_b200(v, Ainds, bb::B200Basis, complex_phases::Bool)
+
+EDKit's `schmidt(v, Ainds, b)` (Schmidt.jl:186-336) on the GPU for the basis
+uploaded as `bb`; `complex_phases` = `eltype(b) <: Complex`.
+"""
+function schmidt_b200(v::Vector{T}, Ainds::AbstractVector{<:Integer}, bb::B200Basis,
+                      complex_phases::Bool, L::Integer) where {T<:Union{Float64,ComplexF64}}
+    a = Int32.(Ainds)
+    cm = T <: Complex || complex_phases
+    M = zeros(cm ? ComplexF64 : Float64, 2^length(a), 2^(L - length(a)))
+    GC.@preserve v a M check(ccall((:edk_schmidt, libedk), Cint,
+        (Ptr{Cvoid}, Int32, Ptr{Cvoid}, Int32, Ptr{Int32}, Ptr{Cvoid}, Int32, Int32),
+        bb.h, _vdt(v), v, length(a), a, M, cm ? 1 : 0, 0))
+    M
+end
+
+"""
+    ent_S_b200(v, Aind, bb::B200Basis; α=1, cutoff=1e-20)
+
+EDKit's `ent_S` (Schmidt.jl:150-153) with the Schmidt matrix and its spectrum
+on the GPU.
+"""
+function ent_S_b200(v::Vector{T}, Aind::AbstractVector{<:Integer}, bb::B200Basis;
+                    α::Real=1, cutoff::Real=1e-20) where {T<:Union{Float64,ComplexF64}}
+    a = Int32.(Aind)
+    S = Ref{Float64}(0.0)
+    GC.@preserve v a check(ccall((:edk_ent_S, libedk), Cint,
+        (Ptr{Cvoid}, Int32, Ptr{Cvoid}, Int32, Ptr{Int32}, Float64, Float64, Ref{Float64}, Int32),
+        bb.h, _vdt(v), v, length(a), a, α, cutoff, S, 0))
+    iszero(α) ? round(Int, S[]) : S[]
+end
+
+"""
+    double_basis_b200(B1::B200Basis, B2::B200Basis, D1, v)
+
+`(DoubleBasis(B1, B2))(v)` (LinearMap.jl:140-166) on the GPU; returns a
+ComplexF64 vector of length `D1 = size(B1, 1)`.
+"""
+function double_basis_b200(B1::B200Basis, B2::B200Basis, D1::Integer,
+                           v::Vector{T}) where {T<:Union{Float64,ComplexF64}}
+    out = zeros(ComplexF64, D1)
+    GC.@preserve v out check(ccall((:edk_double_basis_apply, libedk), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int32, Ptr{Cvoid}, Ptr{ComplexF64}, Int32),
+        B1.h, B2.h, _vdt(v), v, out, 0))
+    out
+end
+
+"""
+    symmetrizer_b200(B1::B200Basis, B2::B200Basis, D1, D2)
+
+`symmetrizer(DoubleBasis(B1, B2))` (LinearMap.jl:183-185) on the GPU.
+"""
+function symmetrizer_b200(B1::B200Basis, B2::B200Basis, D1::Integer, D2::Integer)
+    M = zeros(ComplexF64, D1, D2)
+    GC.@preserve M check(ccall((:edk_symmetrizer, libedk), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{ComplexF64}, Int32), B1.h, B2.h, M, 0))
+    M
+end
 
 end # module
