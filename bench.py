@@ -65,9 +65,10 @@ def measured_peak():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic():
+def profiled_traffic(search="rank"):
     """dram bytes per launch of the matvec kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_apply_trans0_L28_f64.md")
+    name = "k_apply_ff_rank_L28_f64.md" if search == "rank" else "k_apply_trans0_L28_f64.md"
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
@@ -134,9 +135,10 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
-def build_problem(ek):
+def build_problem(ek, search="rank"):
     b = ek.TranslationalBasis(L=L, N=N, k=K_MOM)
     H = ek.trans_inv_operator(ek.spin((1.0, "xx"), (1.0, "yy"), (DELTA, "zz")), 2, b)
+    b.set_search(search)  # index search of the target rows (the autotuner's pick here: rank)
     return b, H
 
 
@@ -152,7 +154,7 @@ def run_gpu(args):
     ek = ge.load_package()
     from edkit_b200 import _lib as E
     lib = E.load()
-    b, H = build_problem(ek)
+    b, H = build_problem(ek, args.search)
     D = b.size(1)
     balg, nnz = algorithmic_bytes(b.I - 1, L)
     dev = torch.device("cuda", local)
@@ -194,6 +196,29 @@ def run_gpu(args):
     ms_step = float(t_max.item())
     value = balg * world / (ms_step * 1e-3) / 1e9
     achieved = balg / (ms_mean * 1e-3) / 1e9
+
+    # the same kernel with the hash-table search, for comparison
+    other = None
+    if args.search != "hash":
+        b.set_search("hash")
+        for _ in range(3):
+            flush.fill_(1.0)
+            matvec()
+        torch.cuda.synchronize()
+        n_o = min(args.steps, 200)
+        evo = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(n_o)]
+        for i in range(n_o):
+            flush.fill_(float(i))
+            evo[i][0].record(stream)
+            matvec()
+            evo[i][1].record(stream)
+        torch.cuda.synchronize()
+        ms_h = float(np.mean([a.elapsed_time(c) for a, c in evo]))
+        other = {"search": "hash", "ms_per_step": round(ms_h, 5),
+                 "GB_s_algorithmic": round(balg / (ms_h * 1e-3) / 1e9, 2),
+                 "speedup_of_headline_search": round(ms_h / ms_mean, 3)}
+        b.set_search(args.search)
 
     # the same product from the cached matrix (sparse!(opt) on the device)
     mat = None
@@ -290,7 +315,7 @@ def run_gpu(args):
     result = None
     if rank == 0:
         peak, src = measured_peak()
-        traffic = profiled_traffic()
+        traffic = profiled_traffic(args.search)
         result = {
             "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 5),
@@ -298,6 +323,7 @@ def run_gpu(args):
             "data": "synthetic (seeded normal psi)",
             "config": {"workload": WORKLOAD, "D": D, "nnz_hits": nnz,
                        "algorithmic_bytes_per_step": balg,
+                       "index_search": args.search,
                        "parallelism": f"replicas{world}",
                        "l2": "flushed between steps (256 MiB write)",
                        "wall_s_timed_region": round(wall, 4)},
@@ -310,6 +336,8 @@ def run_gpu(args):
             "clocks": clk.summary(),
             "check_rel_err_vs_second_run": err,
         }
+        if other is not None:
+            result["matvec_other_search"] = other
         if mat is not None:
             result["matvec_materialized"] = mat
         if blk is not None:
@@ -490,6 +518,7 @@ def config3_krylov(ek, ntimes=101):
     b = ek.TranslationalBasis(L=32, N=16, k=0)
     H = ek.trans_inv_operator(ek.spin((1.0, "xx"), (1.0, "yy"), (1.0, "zz")), 2, b) + \
         ek.trans_inv_operator(ek.spin((0.5, "xx"), (0.5, "yy"), (0.5, "zz")), [1, 3], b)
+    b.set_search("rank")  # 2.4 GB rank table: the fastest matrix-free search here
     rng = np.random.default_rng(99)
     dg = np.zeros(32, dtype=np.int64)
     dg[rng.choice(32, 16, replace=False)] = 1
@@ -619,6 +648,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--search", default="rank", choices=["rank", "hash", "sorted"],
+                    help="index search of the target rows (rank table, hash table, sorted array)")
     ap.add_argument("--skip-e0", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-materialized", action="store_true")

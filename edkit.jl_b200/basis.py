@@ -77,15 +77,18 @@ class AbstractBasis:
                 pass
 
     def set_search(self, strategy):
-        """Index search of a basis with representatives: "hash" (table) or
+        """Index search of a basis with representatives: "hash" (table),
         "sorted" (binary search over the ascending representatives, as
-        EDKit's index() does); rows and results are identical."""
-        E.check(E.load().edk_basis_set_search(self._h, {"hash": 0, "sorted": 1}[strategy]))
+        EDKit's index() does) or "rank" (phase-free translation sectors with
+        fixed N: a table over the charge sector indexed by colex rank, read by
+        the bond-family row kernel); rows and results are identical."""
+        E.check(E.load().edk_basis_set_search(self._h, {"hash": 0, "sorted": 1,
+                                                         "rank": 2}[strategy]))
 
     def get_search(self):
         v = C.c_int32()
         E.check(E.load().edk_basis_get_search(self._h, C.byref(v)))
-        return {0: "hash", 1: "sorted"}[v.value]
+        return {0: "hash", 1: "sorted", 2: "rank"}[v.value]
 
     # --- AbstractBasis interface (AbstractBasis.jl:95-176) ---
     def size(self, dim=None):

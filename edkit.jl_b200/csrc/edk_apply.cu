@@ -84,11 +84,13 @@ edk_status launch_apply_ff(const BasisDev& b, const OpDev& op, const FFParams& f
     k_apply_ff<BK, VT, TPS><<<grid, 256, 0, st>>>(b, op, ff, Xk, Yk, ldx, ldy, accumulate, \
                                                   tile0);                                     \
     break;
-    switch (b.bk) {
+    const int kind = (b.bk == BK_TRANS0 && b.search == 2) ? (int)BK_TRANS0_RANK : b.bk;
+    switch (kind) {
       EDK_FF(BK_TENSOR)
       EDK_FF(BK_PROJ_RANK)
       EDK_FF(BK_PROJ_HASH)
       EDK_FF(BK_TRANS0)
+      EDK_FF(BK_TRANS0_RANK)
       EDK_FF(BK_TRANS)
       EDK_FF(BK_TRANSPAR)
       default:

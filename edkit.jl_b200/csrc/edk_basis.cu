@@ -336,6 +336,38 @@ __global__ void k_index(BasisDev b, int64_t n, const uint64_t* states, int64_t* 
   }
 }
 
+// every representative has popcount K (flag stays 0)
+__global__ void k_popc_check(const uint64_t* I, int64_t D, int K, int* flag) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < D;
+       i += (int64_t)gridDim.x * blockDim.x)
+    if (__popcll(I[i]) != K) *flag = 1;
+}
+// Rank table of a phase-free translation sector: entry r belongs to the state
+// of popcount K with colex rank r (colex unrank: the largest p with
+// C(p, j) <= r for j = K..1), and holds the hash value of its orbit
+// representative or ~0u.  `b` is passed with search = 0 (hash probes).
+__global__ void k_rank_map(BasisDev b, int K, uint64_t n, uint32_t* out) {
+  __shared__ uint32_t sb[32 * 33];
+  for (int q = threadIdx.x; q < 32 * 33; q += blockDim.x) sb[q] = b.binom32[q];
+  __syncthreads();
+  const uint32_t mask = (uint32_t)b.maskL;
+  for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n;
+       r += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t rem = (uint32_t)r, s = 0;
+    int p = b.L - 1;
+    for (int j = K; j >= 1; --j) {
+      while (sb[p * 33 + j] > rem) --p;
+      s |= 1u << p;
+      rem -= sb[p * 33 + j];
+      --p;
+    }
+    const uint32_t key =
+        b.runs_canon ? canon_runs32(s, b.L, mask) : canon_min32(s, b.L, b.A, b.len, mask);
+    uint32_t v;
+    out[r] = hash_find(b, key, v) ? v : ~0u;
+  }
+}
+
 int grid_for(int64_t n, int block = 256, int cap = 148 * 32) {
   int64_t g = (n + block - 1) / block;
   if (g < 1) g = 1;
@@ -853,9 +885,55 @@ extern "C" edk_status edk_basis_create(const edk_basis_desc* desc, edk_basis** o
 
 // Select the index search of a basis with a representative table: the hash
 // table (default) or the two-level binary search over the sorted array.
+namespace {
+// EDK_SEARCH_RANK: build the rank table once (kept until the basis is freed)
+edk_status build_rank_table(edk_basis* b) {
+  if (b->rankmap.p || b->D == 0) return EDK_OK;
+  cudaStream_t st = b->stream;
+  const int L = b->L;
+  uint64_t s0 = 0;
+  EDK_TRY_CUDA(cudaMemcpyAsync(&s0, b->I.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  EDK_TRY_CUDA(cudaStreamSynchronize(st));
+  const int K = __builtin_popcountll(s0);
+  DevBuf flag;
+  EDK_RETURN_IF(flag.alloc(sizeof(int)));
+  EDK_TRY_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+  k_popc_check<<<grid_for(b->D), 256, 0, st>>>(b->I.as<uint64_t>(), b->D, K, flag.as<int>());
+  EDK_TRY_CUDA(cudaGetLastError());
+  int mixed = 0;
+  EDK_TRY_CUDA(cudaMemcpyAsync(&mixed, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  EDK_TRY_CUDA(cudaStreamSynchronize(st));
+  if (mixed) {
+    set_error("edk_basis_set_search: the rank table needs a sector of fixed charge N");
+    return EDK_UNSUPPORTED;
+  }
+  std::vector<uint32_t> binom(32 * 33, 0);
+  for (int p = 0; p < 32; ++p) {
+    binom[p * 33] = 1;
+    for (int k = 1; k <= p; ++k)
+      binom[p * 33 + k] = (p == 0) ? 0 : binom[(p - 1) * 33 + k - 1] + binom[(p - 1) * 33 + k];
+  }
+  uint64_t n = 1;  // C(L, K)
+  for (int k = 1; k <= K; ++k) n = n * (uint64_t)(L - K + k) / (uint64_t)k;
+  EDK_CHECK_ARG(n <= 0xFFFFFFFFull, "edk_basis_set_search: the sector has more than 2^32 states");
+  EDK_RETURN_IF(b->binom32.alloc(binom.size() * sizeof(uint32_t)));
+  EDK_TRY_CUDA(cudaMemcpyAsync(b->binom32.p, binom.data(), binom.size() * sizeof(uint32_t),
+                               cudaMemcpyHostToDevice, st));
+  EDK_RETURN_IF(b->rankmap.alloc(n * sizeof(uint32_t)));
+  BasisDev tmp = b->dev;
+  tmp.search = 0;
+  tmp.binom32 = b->binom32.as<uint32_t>();
+  k_rank_map<<<grid_for((int64_t)n), 256, 0, st>>>(tmp, K, n, b->rankmap.as<uint32_t>());
+  EDK_TRY_CUDA(cudaGetLastError());
+  EDK_TRY_CUDA(cudaStreamSynchronize(st));
+  return EDK_OK;
+}
+}  // namespace
+
 extern "C" edk_status edk_basis_set_search(edk_basis* b, int32_t strategy) {
   EDK_CHECK_ARG(b != nullptr, "edk_basis_set_search: NULL basis");
-  EDK_CHECK_ARG(strategy == EDK_SEARCH_HASH || strategy == EDK_SEARCH_SORTED,
+  EDK_CHECK_ARG(strategy == EDK_SEARCH_HASH || strategy == EDK_SEARCH_SORTED ||
+                    strategy == EDK_SEARCH_RANK,
                 "edk_basis_set_search: unknown strategy");
   std::lock_guard<std::mutex> lk(b->mu);
   const int bk = b->dev.bk;
@@ -866,6 +944,18 @@ extern "C" edk_status edk_basis_set_search(edk_basis* b, int32_t strategy) {
   }
   if (strategy == EDK_SEARCH_HASH) {
     b->dev.search = 0;
+    return EDK_OK;
+  }
+  if (strategy == EDK_SEARCH_RANK) {
+    if (bk != BK_TRANS0 || b->L > 32) {
+      set_error("edk_basis_set_search: the rank table serves phase-free translation sectors "
+                "(TranslationalBasis k = 0) with L <= 32");
+      return EDK_UNSUPPORTED;
+    }
+    EDK_RETURN_IF(build_rank_table(b));
+    b->dev.rankmap = b->rankmap.as<uint32_t>();
+    b->dev.binom32 = b->binom32.as<uint32_t>();
+    b->dev.search = 2;
     return EDK_OK;
   }
   if (!b->keys32.p && !b->fence.p && b->D > 0) {
@@ -911,7 +1001,8 @@ extern "C" edk_status edk_basis_set_search(edk_basis* b, int32_t strategy) {
 
 extern "C" edk_status edk_basis_get_search(const edk_basis* b, int32_t* strategy) {
   EDK_CHECK_ARG(b != nullptr && strategy != nullptr, "edk_basis_get_search: NULL argument");
-  *strategy = b->dev.search ? EDK_SEARCH_SORTED : EDK_SEARCH_HASH;
+  *strategy = b->dev.search == 2 ? EDK_SEARCH_RANK
+               : (b->dev.search == 1 ? EDK_SEARCH_SORTED : EDK_SEARCH_HASH);
   return EDK_OK;
 }
 
@@ -936,10 +1027,12 @@ edk_status check_basis_dev(const BasisDev& b) {
       break;
     default: ok = false;
   }
-  if (ok && b.search && b.bk != BK_TENSOR && b.bk != BK_PROJ_RANK)
+  if (ok && b.search == 1 && b.bk != BK_TENSOR && b.bk != BK_PROJ_RANK)
     ok = (b.L <= 32) ? (b.keys32 != nullptr && b.fence != nullptr) : b.I != nullptr;
-  if (ok && b.search && b.packed && b.bk != BK_TENSOR && b.bk != BK_PROJ_RANK)
+  if (ok && b.search == 1 && b.packed && b.bk != BK_TENSOR && b.bk != BK_PROJ_RANK)
     ok = b.rcls8 != nullptr;
+  if (ok && b.search == 2)
+    ok = b.bk == BK_TRANS0 && b.L <= 32 && b.rankmap != nullptr && b.binom32 != nullptr;
   if (b.D > 0 && !ok) {
     set_error("internal: basis tables missing for its lookup kind");
     return EDK_INVALID_ARG;

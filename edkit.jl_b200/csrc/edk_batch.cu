@@ -535,6 +535,10 @@ struct BatchEngine {
         EDK_BAPPLY(BK_PROJ_RANK)
         EDK_BAPPLY(BK_PROJ_HASH)
         EDK_BAPPLY(BK_TRANS0)
+        case BK_TRANS0_RANK:  // bond-family fast path only (other paths keep the hash)
+          k_bapply_ff<BK_TRANS0_RANK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv,
+                                                                           stp, dn);
+          break;
         EDK_BAPPLY(BK_TRANS)
         EDK_BAPPLY(BK_TRANSPAR)
         default:
@@ -802,6 +806,10 @@ edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczo
     }
     Dmin = std::min<int64_t>(Dmin, op->b->D);
   }
+  // phase-free translation sectors searched through their rank tables
+  bool ranked = bk == BK_TRANS0 && ff;
+  for (auto* op : ops) ranked = ranked && op->b->dev.search == 2;
+  if (ranked) bk = BK_TRANS0_RANK;
   if (bk == BK_ABELIAN && !all_mat) {
     set_error("batch Lanczos: symmetry-group (abelian) bases run one at a time unless materialised");
     return EDK_UNSUPPORTED;

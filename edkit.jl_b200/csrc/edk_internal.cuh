@@ -124,7 +124,10 @@ enum LookupKind : int {
   BK_TRANS0 = 3,     // translation, trivial phase (k = 0): min over rotations
   BK_TRANS = 4,      // translation, phase C[M] from the first-minimum shift M
   BK_TRANSPAR = 5,   // translation + reflection
-  BK_ABELIAN = 6     // generic odometer over commuting generators
+  BK_ABELIAN = 6,    // generic odometer over commuting generators
+  // BK_TRANS0 basis searched through its rank table (EDK_SEARCH_RANK); only
+  // the bond-family fast path instantiates it, every other path keeps the hash
+  BK_TRANS0_RANK = 7
 };
 
 constexpr int kMaxGen = 8;
@@ -166,6 +169,12 @@ struct BasisDev {
   const uint32_t* fence;   // keys32[32 j]: first level of the search
   int64_t nfence;
   const uint8_t* rcls8;    // norm class of each row (packed values), else null
+  // rank table (edk_basis_set_search(EDK_SEARCH_RANK), search == 2): for every
+  // state with the sector's popcount, indexed by its colex rank, the hash value
+  // of its representative (row << 5 | class, or row) or ~0u when the orbit is
+  // not in the basis; binom32[p * 33 + k] = C(p, k) for p < 32
+  const uint32_t* rankmap;
+  const uint32_t* binom32;
   int nclass;
   double Rcls[kNormClasses];
   // BK_PROJ_RANK
@@ -257,6 +266,7 @@ struct edk_basis {
   int64_t D = 0;
   edk::DevBuf I, R, htab, phase, gens;
   edk::DevBuf keys32, fence, rcls8;  // sorted-array search tables (built on demand)
+  edk::DevBuf rankmap, binom32;      // rank table of EDK_SEARCH_RANK (built on demand)
   edk::BasisDev dev{};
   std::vector<edk::GenDev> gens_host;
   std::vector<int> gen_order, gen_q;

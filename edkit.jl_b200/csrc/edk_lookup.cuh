@@ -101,7 +101,7 @@ __device__ __forceinline__ bool sorted_find64(const BasisDev& b, uint64_t key, u
 
 // 32-bit keys: one 8-byte slot = key << 32 | value, empty = all ones.
 __device__ __forceinline__ bool hash_find(const BasisDev& b, uint32_t key, uint32_t& val) {
-  if (b.search) return sorted_find32(b, key, val);
+  if (b.search == 1) return sorted_find32(b, key, val);
   const unsigned long long* tab = reinterpret_cast<const unsigned long long*>(b.htab);
   uint64_t slot = hslot32(key, b.hbits);
   for (uint64_t n = 0; n <= b.hmask; ++n) {
@@ -114,7 +114,7 @@ __device__ __forceinline__ bool hash_find(const BasisDev& b, uint32_t key, uint3
 }
 // 64-bit keys: 16-byte slots {key, value}, empty key = all ones.
 __device__ __forceinline__ bool hash_find(const BasisDev& b, uint64_t key, uint32_t& val) {
-  if (b.search) return sorted_find64(b, key, val);
+  if (b.search == 1) return sorted_find64(b, key, val);
   const ulonglong2* tab = reinterpret_cast<const ulonglong2*>(b.htab);
   uint64_t slot = hmix64(key) & b.hmask;
   for (uint64_t n = 0; n <= b.hmask; ++n) {

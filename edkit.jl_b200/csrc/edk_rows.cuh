@@ -227,7 +227,7 @@ __device__ __forceinline__ void locate2(const BasisDev& b, const uint32_t* s_bin
     p2 = ok2 ? colex_rank(k2, s_binom) : 0;
   } else {
     uint32_t v1 = 0, v2 = 0;
-    if (b.search) {
+    if (b.search == 1) {
       ok1 = sorted_find32(b, k1, v1);
       ok2 = two && sorted_find32(b, k2, v2);
     } else {
@@ -249,6 +249,28 @@ __device__ __forceinline__ void locate2(const BasisDev& b, const uint32_t* s_bin
   }
 }
 
+// Colex rank of s with the set bit and the empty bit at positions p, q
+// exchanged, from the rank rs of s: the moving bit keeps its place among the
+// set bits below min(p, q), the set bits strictly between the two positions
+// shift their index by one.  Adjacent positions cost one table read; the
+// wrap-around bond walks the set bits in between.  binom[p * 33 + k] = C(p, k).
+__device__ __forceinline__ uint32_t rank_after_swap(uint32_t s, uint32_t rs, int p, int q,
+                                                    const uint32_t* binom) {
+  const int a = min(p, q), c = max(p, q);  // a < c <= 31
+  const int j = __popc(s & ((1u << a) - 1u));
+  uint32_t between = s & ((1u << c) - 1u) & ~((2u << a) - 1u);
+  const int nb = __popc(between);
+  // the bit at a moves up to c: C(c, j+1+nb) - C(a, j+1), and every bit in
+  // between drops from index j+1+k to j+k
+  uint32_t delta = binom[c * 33 + j + 1 + nb] - binom[a * 33 + j + 1];
+  for (int k = 1; between; ++k) {
+    const int r = __ffs(between) - 1;
+    between &= between - 1;
+    delta += binom[r * 33 + j + k] - binom[r * 33 + j + 1 + k];
+  }
+  return ((s >> a) & 1u) ? rs + delta : rs - delta;  // modulo 2^32: the result is a valid rank
+}
+
 // 256 / TPS consecutive rows r0.. of the flip-flop fast path (one block of
 // 256 threads).  Rows are sorted by their number of off-diagonal hits so that
 // the lanes of a warp loop equally long; TPS adjacent lanes share one row and
@@ -260,11 +282,17 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
                                         VT* __restrict__ yk, int accumulate) {
   using A = typename VTraits<VT>::A;
   constexpr bool CX = VTraits<VT>::cx;
-  __shared__ uint32_t s_binom[(BK == BK_PROJ_RANK) ? 32 * 33 : 1];
+  // BK_TRANS0_RANK: a phase-free translation sector whose target rows come
+  // from the rank table instead of canonicalisation + hash probe
+  constexpr bool RANKED = BK == BK_TRANS0_RANK;
+  constexpr int BKL = RANKED ? (int)BK_TRANS0 : BK;
+  __shared__ uint32_t s_binom[(BK == BK_PROJ_RANK || RANKED) ? 32 * 33 : 1];
   __shared__ int s_hist[64];
   __shared__ unsigned short s_order[256];
   __shared__ uint32_t s_state[256];
   if constexpr (BK == BK_PROJ_RANK) fill_binom32(s_binom);
+  if constexpr (RANKED)
+    for (int q = threadIdx.x; q < 32 * 33; q += blockDim.x) s_binom[q] = __ldg(b.binom32 + q);
   constexpr int RT = 256 / TPS;  // rows per tile
   const int t = threadIdx.x;
   if (t < 64) s_hist[t] = 0;
@@ -307,6 +335,8 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
   if (TPS == 1 && !valid) return;
   const uint32_t st = s_state[tt];  // 0 past the last row: no hits
   const A invRi = (b.R && valid) ? (A)(1.0 / __ldg(b.R + i)) : (A)1;
+  uint32_t rs = 0;  // colex rank of the row state (rank-table search)
+  if constexpr (RANKED) rs = (uint32_t)colex_rank(st, s_binom);
   int pc = 0;  // pairs of hits seen so far in this row
   double dr = 0.0, di = 0.0;
   A ar = 0, ai = 0;
@@ -339,14 +369,28 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
       if (two) bits &= bits - 1;
       if (TPS > 1 && (pc++ % TPS) != sub) continue;
       const int q1 = p1 >= d ? p1 - d : p1 - d + L, q2 = p2 >= d ? p2 - d : p2 - d + L;
-      const uint32_t s1 = st ^ (1u << p1) ^ (1u << q1), s2 = st ^ (1u << p2) ^ (1u << q2);
       HitCtx h1, h2;
-      canon_ctx<BK>(b, s1, h1);
-      canon_ctx<BK>(b, s2, h2);
       int64_t pos1, pos2;
       double rp1, rp2;
       bool ok1, ok2;
-      locate2<BK>(b, s_binom, h1.key, h2.key, two, pos1, rp1, ok1, pos2, rp2, ok2);
+      if constexpr (RANKED) {
+        h1 = h2 = HitCtx{0u, 1.0, 0.0};
+        const uint32_t k1 = rank_after_swap(st, rs, p1, q1, s_binom);
+        const uint32_t k2 = two ? rank_after_swap(st, rs, p2, q2, s_binom) : k1;
+        const uint32_t v1 = __ldg(b.rankmap + k1);
+        const uint32_t v2 = two ? __ldg(b.rankmap + k2) : ~0u;
+        ok1 = v1 != ~0u;
+        ok2 = v2 != ~0u;
+        pos1 = pos2 = 0;
+        rp1 = rp2 = 1.0;
+        if (ok1) decode_val(b, v1, pos1, rp1);
+        if (ok2) decode_val(b, v2, pos2, rp2);
+      } else {
+        const uint32_t s1 = st ^ (1u << p1) ^ (1u << q1), s2 = st ^ (1u << p2) ^ (1u << q2);
+        canon_ctx<BKL>(b, s1, h1);
+        canon_ctx<BKL>(b, s2, h2);
+        locate2<BKL>(b, s_binom, h1.key, h2.key, two, pos1, rp1, ok1, pos2, rp2, ok2);
+      }
       const Cx<A> x1 = ok1 ? ldv(xk + pos1) : Cx<A>{0, 0};
       const Cx<A> x2 = ok2 ? ldv(xk + pos2) : Cx<A>{0, 0};
       const double2 w1 = ((st >> p1) & 1u) ? vb : va;

@@ -29,6 +29,17 @@ size_t elem_size(int dtype) {
 }
 
 // median time of `reps` back-to-back applications on the operator's stream
+// bytes of the rank table of a phase-free translation sector: 4 * C(L, K)
+size_t rank_table_bytes(edk_basis* b) {
+  uint64_t s0 = 0;
+  if (b->D == 0 || cudaMemcpy(&s0, b->I.p, sizeof(uint64_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return 0;
+  const int L = b->L, K = __builtin_popcountll(s0);
+  uint64_t n = 1;
+  for (int k = 1; k <= K; ++k) n = n * (uint64_t)(L - K + k) / (uint64_t)k;
+  return (size_t)n * 4;
+}
+
 edk_status time_apply(edk_operator* op, int dtype, const void* x, void* y, int64_t nvec,
                       int reps, double& ms) {
   const int64_t D = op->b->D;
@@ -99,7 +110,7 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
   if (D == 0) {
     out.kernel = op->use_ff && op->ff_ok ? EDK_KERNEL_FAST : EDK_KERNEL_GENERIC;
     out.tps = op->tps;
-    out.search = b->dev.search ? EDK_SEARCH_SORTED : EDK_SEARCH_HASH;
+    edk_basis_get_search(b, &out.search);
     if (res) *res = out;
     return EDK_OK;
   }
@@ -114,6 +125,15 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
   std::vector<int> searches{EDK_SEARCH_HASH};
   if (has_search && edk_basis_set_search(b, EDK_SEARCH_SORTED) == EDK_OK)
     searches.push_back(EDK_SEARCH_SORTED);
+  // the rank table (4 bytes per state of the charge sector) when it applies
+  // and takes at most a quarter of the free memory
+  if (has_search && op->ff_ok && op->gather && b->dev.bk == BK_TRANS0 && b->L <= 32) {
+    size_t freeb = 0, totalb = 0;
+    if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess &&
+        (b->rankmap.p || rank_table_bytes(b) <= freeb / 4) &&
+        edk_basis_set_search(b, EDK_SEARCH_RANK) == EDK_OK)
+      searches.push_back(EDK_SEARCH_RANK);
+  }
   struct Cand { int kernel, search, tps, block; };
   std::vector<Cand> cands;
   const bool fast = op->ff_ok && op->gather;
@@ -123,6 +143,7 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
   for (int s : searches) {
     if (fast)
       for (int t : {1, 2, 4}) cands.push_back({EDK_KERNEL_FAST, s, t, 0});
+    if (s == EDK_SEARCH_RANK) continue;  // only the bond-family row kernel reads the rank table
     if (fast && multi && op->b->dev.L <= 32) cands.push_back({EDK_KERNEL_FAST, s, 1, 1});
     cands.push_back({EDK_KERNEL_GENERIC, s, 1, 0});
   }
@@ -182,7 +203,7 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
     op->sell_tma = pick.kernel == EDK_KERNEL_MATERIALIZED_STAGED;
   }
   out.kernel = pick.kernel;
-  out.search = b->dev.search ? EDK_SEARCH_SORTED : EDK_SEARCH_HASH;
+  edk_basis_get_search(b, &out.search);
   out.tps = pick_free.tps;
   out.block = pick.block;
   out.ms = best;

@@ -313,7 +313,7 @@ class Operator:
                                                 E.TUNE_MATERIALIZE if materialize else 0,
                                                 C.byref(r)))
         names = {v: k for k, v in self._KERNELS.items()}
-        srch = {0: "hash", 1: "sorted"}
+        srch = {0: "hash", 1: "sorted", 2: "rank"}
         self.materialized = r.kernel in (E.KERNEL_MATERIALIZED, E.KERNEL_MATERIALIZED_STAGED)
         return {"kernel": names[r.kernel], "search": srch[r.search], "tps": r.tps,
                 "block": bool(r.block), "ms": r.ms,

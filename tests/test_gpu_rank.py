@@ -1,0 +1,109 @@
+"""The rank-table index search (EDK_SEARCH_RANK) of phase-free translation
+sectors: the bond-family row kernel finds target rows by updating the colex
+rank of the row state and reading one table entry.  Rows are the ones EDKit's
+index() gives, so H*x must equal the hash-table result bit for bit and the
+oracle's mul within 1e-12 (FP64)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+XXZ = ((1.0, "xx"), (1.0, "yy"), (1.5, "zz"))
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300)
+
+
+def j1j2(ek, L, b, h=None):
+    mats = [ek.spin(*XXZ)] * L + [ek.spin((0.5, "xx"), (0.5, "yy"), (0.5, "zz"))] * L
+    inds = [[i, i % L + 1] for i in range(1, L + 1)] + [[i, (i + 1) % L + 1] for i in range(1, L + 1)]
+    if h is not None:
+        mats += [h * ek.spin("z")] * L
+        inds += [[i] for i in range(1, L + 1)]
+    return ek.operator(mats, inds, b)
+
+
+def pxp(d):
+    return all(not (d[i] == 1 and d[(i + 1) % len(d)] == 1) for i in range(len(d)))
+
+
+@pytest.mark.parametrize("L,N", [(12, 6), (16, 8), (16, 5), (20, 10), (24, 12)])
+def test_rank_search_bit_exact_with_hash(ek, O, L, N):
+    rng = np.random.default_rng(L + N)
+    b = ek.TranslationalBasis(L=L, k=0, N=N)
+    ops = [("xxz", ek.trans_inv_operator(ek.spin(*XXZ), 2, b)),
+           ("j1j2+h", j1j2(ek, L, b, h=0.3))]
+    D = b.size(1)
+    for name, H in ops:
+        for dt in (np.float64, np.complex128, np.float32):
+            x = rng.standard_normal(D).astype(dt)
+            if np.iscomplexobj(x):
+                x = x + 1j * rng.standard_normal(D)
+            for tps in (1, 2, 4):
+                H.configure_("fast", tps)
+                b.set_search("hash")
+                y_hash = H * x
+                b.set_search("rank")
+                assert b.get_search() == "rank"
+                y_rank = H * x
+                assert np.array_equal(y_rank, y_hash), (name, dt, tps)
+        b.set_search("hash")
+    if L <= 16:  # and against the oracle
+        o = O.translational(L, k=0, N=N)
+        Ho = O.trans_inv_operator(O.spin(*XXZ), 2, o)
+        x = rng.standard_normal(D)
+        b.set_search("rank")
+        H = ops[0][1]
+        H.configure_("fast", 1)
+        assert rel(H * x, Ho.mul(x).real) < 1e-12
+
+
+def test_rank_search_with_predicate_and_unit_cell_rejected(ek, O):
+    """A predicate drops states (their table entries stay empty); bases the
+    table does not serve are refused with EDK_UNSUPPORTED."""
+    L = 14
+    b = ek.TranslationalBasis(L=L, k=0, N=9, f=pxp)  # 5 up spins, no two adjacent
+    o = O.translational(L, k=0, N=9, f=pxp)
+    assert b.size(1) == o.dim > 0
+    H = ek.trans_inv_operator(ek.spin(*XXZ), 2, b)
+    Ho = O.trans_inv_operator(O.spin(*XXZ), 2, o)
+    x = np.random.default_rng(3).standard_normal(b.size(1))
+    b.set_search("rank")
+    H.configure_("fast", 1)
+    assert rel(H * x, Ho.mul(x).real) < 1e-12
+    for bad in (ek.TranslationalBasis(L=L, k=1, N=7), ek.TranslationalBasis(L=L, k=0),
+                ek.TranslationParityBasis(L=L, k=0, p=1, N=7)):
+        with pytest.raises(ek.EDKError):
+            bad.set_search("rank")
+
+
+def test_rank_search_lanczos_and_batches(ek, O):
+    L = 16
+    rng = np.random.default_rng(5)
+    refs, ops = [], []
+    for N in (7, 8):
+        b = ek.TranslationalBasis(L=L, k=0, N=N)
+        o = O.translational(L, k=0, N=N)
+        b.set_search("rank")
+        ops.append(ek.trans_inv_operator(ek.spin(*XXZ), 2, b))
+        refs.append(np.linalg.eigvalsh(O.trans_inv_operator(O.spin(*XXZ), 2, o).dense())[:2])
+    e, _ = ek.lanczos_e0(ops[1], rng.standard_normal(ops[1].size(1)), m=120, tol=1e-13)
+    assert abs(e[0] - refs[1][0]) < 1e-11 * abs(refs[1][0])
+    ev, _ = ek.batch_lanczos_e0(ops, m=120, nev=2, tol=1e-13, check_every=5)
+    for q in range(2):
+        assert np.allclose(ev[q], refs[q], rtol=0, atol=1e-10 * abs(refs[q][0])), q
+
+
+def test_autotune_offers_rank_search(ek, O):
+    L = 18
+    b = ek.TranslationalBasis(L=L, k=0, N=9)
+    o = O.translational(L, k=0, N=9)
+    H = ek.trans_inv_operator(ek.spin(*XXZ), 2, b)
+    Ho = O.trans_inv_operator(O.spin(*XXZ), 2, o)
+    r = H.autotune_()
+    kinds = {(k, s, t) for k, s, t, _ in r["candidates"]}
+    assert ("fast", "rank", 1) in kinds
+    assert b.get_search() == r["search"]
+    x = np.random.default_rng(6).standard_normal(b.size(1))
+    assert rel(H * x, Ho.mul(x).real) < 1e-12
