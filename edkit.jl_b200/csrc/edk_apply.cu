@@ -24,6 +24,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <type_traits>
 
 #include "edk_spmm.cuh"
 
@@ -46,8 +47,18 @@ __global__ void __launch_bounds__(256) k_apply(BasisDev b, OpDev op, const VT* _
     gen_row<BK, S, VT, GATHER>(b, op, i, xk, yk, accumulate, s_binom);
 }
 
+// Resident blocks per SM asked of the compiler: the rank-search kernel is
+// latency bound and fits 32 registers for real and single-precision complex
+// vectors (8 blocks of 256 threads fill every warp slot); the others keep the
+// compiler's choice.
+template <int BK, class VT>
+constexpr int ff_min_blocks() {
+  return (BK == BK_TRANS0_RANK && !std::is_same<VT, double2>::value) ? 8 : 1;
+}
+
 template <int BK, class VT, int TPS>
-__global__ void __launch_bounds__(256) k_apply_ff(BasisDev b, OpDev op, FFParams ff,
+__global__ void __launch_bounds__(256, ff_min_blocks<BK, VT>())
+    k_apply_ff(BasisDev b, OpDev op, FFParams ff,
                                                   const VT* __restrict__ x, VT* __restrict__ y,
                                                   int64_t ldx, int64_t ldy, int accumulate,
                                                   int64_t tile0) {

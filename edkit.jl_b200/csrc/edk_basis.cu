@@ -368,6 +368,13 @@ __global__ void k_rank_map(BasisDev b, int K, uint64_t n, uint32_t* out) {
   }
 }
 
+// colex rank of every representative (the row states of the rank search)
+__global__ void k_row_rank(const uint64_t* I, int64_t D, const uint32_t* binom, uint32_t* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < D;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (uint32_t)colex_rank((uint32_t)I[i], binom);
+}
+
 int grid_for(int64_t n, int block = 256, int cap = 148 * 32) {
   int64_t g = (n + block - 1) / block;
   if (g < 1) g = 1;
@@ -925,6 +932,10 @@ edk_status build_rank_table(edk_basis* b) {
   tmp.binom32 = b->binom32.as<uint32_t>();
   k_rank_map<<<grid_for((int64_t)n), 256, 0, st>>>(tmp, K, n, b->rankmap.as<uint32_t>());
   EDK_TRY_CUDA(cudaGetLastError());
+  EDK_RETURN_IF(b->rowrank.alloc(b->D * sizeof(uint32_t)));
+  k_row_rank<<<grid_for(b->D), 256, 0, st>>>(b->I.as<uint64_t>(), b->D, b->binom32.as<uint32_t>(),
+                                             b->rowrank.as<uint32_t>());
+  EDK_TRY_CUDA(cudaGetLastError());
   EDK_TRY_CUDA(cudaStreamSynchronize(st));
   return EDK_OK;
 }
@@ -955,6 +966,7 @@ extern "C" edk_status edk_basis_set_search(edk_basis* b, int32_t strategy) {
     EDK_RETURN_IF(build_rank_table(b));
     b->dev.rankmap = b->rankmap.as<uint32_t>();
     b->dev.binom32 = b->binom32.as<uint32_t>();
+    b->dev.rowrank = b->rowrank.as<uint32_t>();
     b->dev.search = 2;
     return EDK_OK;
   }
@@ -1032,7 +1044,8 @@ edk_status check_basis_dev(const BasisDev& b) {
   if (ok && b.search == 1 && b.packed && b.bk != BK_TENSOR && b.bk != BK_PROJ_RANK)
     ok = b.rcls8 != nullptr;
   if (ok && b.search == 2)
-    ok = b.bk == BK_TRANS0 && b.L <= 32 && b.rankmap != nullptr && b.binom32 != nullptr;
+    ok = b.bk == BK_TRANS0 && b.L <= 32 && b.rankmap != nullptr && b.binom32 != nullptr &&
+         b.rowrank != nullptr;
   if (b.D > 0 && !ok) {
     set_error("internal: basis tables missing for its lookup kind");
     return EDK_INVALID_ARG;

@@ -175,6 +175,7 @@ struct BasisDev {
   // not in the basis; binom32[p * 33 + k] = C(p, k) for p < 32
   const uint32_t* rankmap;
   const uint32_t* binom32;
+  const uint32_t* rowrank;   // colex rank of each representative I[i]
   int nclass;
   double Rcls[kNormClasses];
   // BK_PROJ_RANK
@@ -266,7 +267,7 @@ struct edk_basis {
   int64_t D = 0;
   edk::DevBuf I, R, htab, phase, gens;
   edk::DevBuf keys32, fence, rcls8;  // sorted-array search tables (built on demand)
-  edk::DevBuf rankmap, binom32;      // rank table of EDK_SEARCH_RANK (built on demand)
+  edk::DevBuf rankmap, binom32, rowrank;  // rank table of EDK_SEARCH_RANK (built on demand)
   edk::BasisDev dev{};
   std::vector<edk::GenDev> gens_host;
   std::vector<int> gen_order, gen_q;

@@ -336,7 +336,7 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
   const uint32_t st = s_state[tt];  // 0 past the last row: no hits
   const A invRi = (b.R && valid) ? (A)(1.0 / __ldg(b.R + i)) : (A)1;
   uint32_t rs = 0;  // colex rank of the row state (rank-table search)
-  if constexpr (RANKED) rs = (uint32_t)colex_rank(st, s_binom);
+  if constexpr (RANKED) rs = valid ? __ldg(b.rowrank + i) : 0u;
   int pc = 0;  // pairs of hits seen so far in this row
   double dr = 0.0, di = 0.0;
   A ar = 0, ai = 0;
@@ -375,8 +375,19 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
       bool ok1, ok2;
       if constexpr (RANKED) {
         h1 = h2 = HitCtx{0u, 1.0, 0.0};
-        const uint32_t k1 = rank_after_swap(st, rs, p1, q1, s_binom);
-        const uint32_t k2 = two ? rank_after_swap(st, rs, p2, q2, s_binom) : k1;
+        uint32_t k1, k2;
+        if (d == 1 && p1 != 0) {
+          // adjacent sites (p2 >= p1 > 0, no wrap-around): the bit at a = p - 1
+          // moves by one place, rank change C(a, j) with j set bits below a
+          const int a1 = p1 - 1, a2 = p2 - 1;
+          const uint32_t e1 = s_binom[a1 * 33 + __popc(st & ((1u << a1) - 1u))];
+          const uint32_t e2 = s_binom[a2 * 33 + __popc(st & ((1u << a2) - 1u))];
+          k1 = ((st >> a1) & 1u) ? rs + e1 : rs - e1;
+          k2 = ((st >> a2) & 1u) ? rs + e2 : rs - e2;
+        } else {
+          k1 = rank_after_swap(st, rs, p1, q1, s_binom);
+          k2 = two ? rank_after_swap(st, rs, p2, q2, s_binom) : k1;
+        }
         const uint32_t v1 = __ldg(b.rankmap + k1);
         const uint32_t v2 = two ? __ldg(b.rankmap + k2) : ~0u;
         ok1 = v1 != ~0u;
