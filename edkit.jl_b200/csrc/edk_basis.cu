@@ -895,7 +895,10 @@ extern "C" edk_status edk_basis_create(const edk_basis_desc* desc, edk_basis** o
 namespace {
 // EDK_SEARCH_RANK: build the rank table once (kept until the basis is freed)
 edk_status build_rank_table(edk_basis* b) {
-  if (b->rankmap.p || b->D == 0) return EDK_OK;
+  if ((b->rankmap.p && b->rowrank.p) || b->D == 0) return EDK_OK;
+  // a build that failed part-way (out of memory) starts again from nothing
+  b->rankmap.release();
+  b->rowrank.release();
   cudaStream_t st = b->stream;
   const int L = b->L;
   uint64_t s0 = 0;

@@ -107,3 +107,43 @@ def test_autotune_offers_rank_search(ek, O):
     assert b.get_search() == r["search"]
     x = np.random.default_rng(6).standard_normal(b.size(1))
     assert rel(H * x, Ho.mul(x).real) < 1e-12
+
+
+@pytest.mark.parametrize("nvec", [5, 64])
+def test_rank_search_spmm_bit_exact_with_hash(ek, nvec):
+    """Several right-hand sides through one SpMM (which locates rows through
+    the hash table whatever the basis' search: there the psi rows, not the
+    lookups, set the time): the same block product under either search."""
+    L = 20
+    b = ek.TranslationalBasis(L=L, k=0, N=10)
+    H = j1j2(ek, L, b, h=0.2)
+    rng = np.random.default_rng(nvec)
+    X = np.asfortranarray(rng.standard_normal((b.size(1), nvec)))
+    H.configure_("fast", 1, block=True)
+    b.set_search("hash")
+    Y_hash = H * X
+    b.set_search("rank")
+    Y_rank = H * X
+    assert np.array_equal(Y_rank, Y_hash)
+    H.configure_("fast", 1, block=False)
+    assert rel(H * X, Y_hash) < 1e-14
+    b.set_search("hash")
+
+
+def test_block_lanczos_mixes_ranked_and_phased_sectors(ek, O):
+    """A block Lanczos batch with a rank-searched k = 0 sector beside k != 0
+    sectors runs on the shared translation path and finds the sectors' levels."""
+    L = 14
+    ops, refs = [], []
+    for k in (0, 1, 7):
+        b = ek.TranslationalBasis(L=L, k=k, N=7)
+        if k == 0:
+            b.set_search("rank")
+        ops.append(ek.trans_inv_operator(ek.spin(*XXZ), 2, b))
+        Ho = O.trans_inv_operator(O.spin(*XXZ), 2, O.translational(L, k=k, N=7))
+        w = np.linalg.eigvalsh(Ho.dense())
+        distinct = [w[0]] + [x for a, x in zip(w[:-1], w[1:]) if x - a > 1e-8 * abs(w[0])]
+        refs.append(distinct[:3])
+    ev, _ = ek.block_lanczos(ops, block=8, m=24, nev=3, check_every=0)
+    for q in range(3):
+        assert np.allclose(ev[q][:3], refs[q], rtol=0, atol=1e-9 * abs(refs[q][0])), q
