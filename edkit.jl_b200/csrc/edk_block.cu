@@ -511,14 +511,8 @@ static edk_status block_lanczos(int nops, edk_operator* const* ops,
     if (kind == 2) any_generic = true;
     if (kind == 0) {
       if (bk_ff >= 0 && bk_ff != bk) {
-        // translation sectors with and without the rank table share the hash path
-        const bool trans = (bk_ff == BK_TRANS || bk_ff == BK_TRANS0_RANK) &&
-                           (bk == BK_TRANS || bk == BK_TRANS0_RANK);
-        if (!trans) {
-          set_error("edk_block_lanczos: operators on different kinds of basis in one batch");
-          return EDK_UNSUPPORTED;
-        }
-        bk = BK_TRANS;
+        set_error("edk_block_lanczos: operators on different kinds of basis in one batch");
+        return EDK_UNSUPPORTED;
       }
       bk_ff = bk;
     }

@@ -126,12 +126,8 @@ __global__ void __launch_bounds__(256) k_spmm_ff(const SpmmOp* __restrict__ ops,
                                                  const VT* __restrict__ X, VT* __restrict__ Y,
                                                  int accumulate) {
   using A = typename VTraits<VT>::A;
-  // BK_TRANS0_RANK: target rows from the rank table (phase-free translation
-  // sectors), no canonicalisation
-  constexpr bool RANKED = BK == BK_TRANS0_RANK;
-  constexpr int BKL = RANKED ? (int)BK_TRANS0 : BK;
-  __shared__ uint32_t s_binom[(BK == BK_PROJ_RANK || RANKED) ? 32 * 33 : 1];
-  if constexpr (BK == BK_PROJ_RANK || RANKED) {
+  __shared__ uint32_t s_binom[(BK == BK_PROJ_RANK) ? 32 * 33 : 1];
+  if constexpr (BK == BK_PROJ_RANK) {
     fill_binom32(s_binom);
     __syncthreads();
   }
@@ -149,8 +145,6 @@ __global__ void __launch_bounds__(256) k_spmm_ff(const SpmmOp* __restrict__ ops,
     const uint32_t mask = (uint32_t)b.maskL;
     const uint32_t st = (BK == BK_TENSOR) ? (uint32_t)i : (uint32_t)__ldg(b.I + i);
     const double invRi = b.R ? 1.0 / __ldg(b.R + i) : 1.0;
-    uint32_t rs = 0;  // colex rank of the row state (rank-table search)
-    if constexpr (RANKED) rs = __ldg(b.rowrank + i);
     uint32_t hm[kMaxFF];
     int cnt[kMaxFF];
     int nhit = 0;
@@ -195,20 +189,11 @@ __global__ void __launch_bounds__(256) k_spmm_ff(const SpmmOp* __restrict__ ops,
         const int d = ff.d[f];
         const int qb = pb >= d ? pb - d : pb - d + b.L;
         HitCtx h;
+        canon_ctx<BK>(b, st ^ (1u << pb) ^ (1u << qb), h);
         int64_t p1, p2;
         double r1, r2;
         bool ok1, ok2;
-        if constexpr (RANKED) {
-          h = HitCtx{0u, 1.0, 0.0};
-          const uint32_t v = __ldg(b.rankmap + rank_after_swap(st, rs, pb, qb, s_binom));
-          ok1 = v != ~0u;
-          p1 = 0;
-          r1 = 1.0;
-          if (ok1) decode_val(b, v, p1, r1);
-        } else {
-          canon_ctx<BKL>(b, st ^ (1u << pb) ^ (1u << qb), h);
-          locate2<BKL>(b, s_binom, h.key, h.key, false, p1, r1, ok1, p2, r2, ok2);
-        }
+        locate2<BK>(b, s_binom, h.key, h.key, false, p1, r1, ok1, p2, r2, ok2);
         if (ok1) {
           const double2 w = ((st >> pb) & 1u) ? ff.v2[f] : ff.v1[f];
           const double ratio = r1 * invRi;
@@ -309,7 +294,6 @@ edk_status launch_spmm(const SpmmOp* d_ops, int nops, int bk_ff, int64_t smax, i
       EDK_SPMM_FF(BK_PROJ_RANK)
       EDK_SPMM_FF(BK_PROJ_HASH)
       EDK_SPMM_FF(BK_TRANS)
-      EDK_SPMM_FF(BK_TRANS0_RANK)
       EDK_SPMM_FF(BK_TRANSPAR)
       default:
         set_error("SpMM: unsupported basis kind for the bond-family kernel");
@@ -346,8 +330,7 @@ inline int spmm_describe(const edk_operator* op, SpmmOp& h, int& bk, int64_t& sl
   } else if (op->ff_ok && op->use_ff && op->b->dev.L <= 32) {
     h.kind = 0;
     std::memcpy(&h.ff, op->ff_params.data(), sizeof(FFParams));
-    const BasisDev& bd = op->b->dev;
-    bk = bd.bk == BK_TRANS0 ? (bd.search == 2 ? (int)BK_TRANS0_RANK : (int)BK_TRANS) : bd.bk;
+    bk = op->b->dev.bk == BK_TRANS0 ? BK_TRANS : op->b->dev.bk;
     h.b.bk = bk;
   } else {
     h.kind = 2;
