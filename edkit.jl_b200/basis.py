@@ -79,9 +79,9 @@ class AbstractBasis:
     def set_search(self, strategy):
         """Index search of a basis with representatives: "hash" (table),
         "sorted" (binary search over the ascending representatives, as
-        EDKit's index() does) or "rank" (phase-free translation sectors with
-        fixed N: a table over the charge sector indexed by colex rank, read by
-        the bond-family row kernel); rows and results are identical."""
+        EDKit's index() does) or "rank" (translation sectors of fixed N: a
+        table over the charge sector indexed by colex rank, read by the
+        bond-family row kernel); rows and results are identical."""
         E.check(E.load().edk_basis_set_search(self._h, {"hash": 0, "sorted": 1,
                                                          "rank": 2}[strategy]))
 

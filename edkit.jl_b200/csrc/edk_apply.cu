@@ -47,13 +47,16 @@ __global__ void __launch_bounds__(256) k_apply(BasisDev b, OpDev op, const VT* _
     gen_row<BK, S, VT, GATHER>(b, op, i, xk, yk, accumulate, s_binom);
 }
 
-// Resident blocks per SM asked of the compiler: the rank-search kernel is
-// latency bound and fits 32 registers for real and single-precision complex
-// vectors (8 blocks of 256 threads fill every warp slot); the others keep the
-// compiler's choice.
+// Resident blocks per SM asked of the compiler: the rank-search kernels are
+// latency bound and fit 32 registers (8 blocks of 256 threads fill every warp
+// slot) for real and single-precision complex vectors, or single precision
+// when the sector has a phase; the others keep the compiler's choice.
 template <int BK, class VT>
 constexpr int ff_min_blocks() {
-  return (BK == BK_TRANS0_RANK && !std::is_same<VT, double2>::value) ? 8 : 1;
+  return (BK == BK_TRANS0_RANK && !std::is_same<VT, double2>::value) ||
+                 (BK == BK_TRANS_RANK && (std::is_same<VT, float>::value ||
+                                          std::is_same<VT, float2>::value))
+             ? 8 : 1;
 }
 
 template <int BK, class VT, int TPS>
@@ -95,13 +98,16 @@ edk_status launch_apply_ff(const BasisDev& b, const OpDev& op, const FFParams& f
     k_apply_ff<BK, VT, TPS><<<grid, 256, 0, st>>>(b, op, ff, Xk, Yk, ldx, ldy, accumulate, \
                                                   tile0);                                     \
     break;
-    const int kind = (b.bk == BK_TRANS0 && b.search == 2) ? (int)BK_TRANS0_RANK : b.bk;
+    const int kind = b.search != 2 ? b.bk
+                     : (b.bk == BK_TRANS0 ? (int)BK_TRANS0_RANK
+                                          : (b.bk == BK_TRANS ? (int)BK_TRANS_RANK : b.bk));
     switch (kind) {
       EDK_FF(BK_TENSOR)
       EDK_FF(BK_PROJ_RANK)
       EDK_FF(BK_PROJ_HASH)
       EDK_FF(BK_TRANS0)
       EDK_FF(BK_TRANS0_RANK)
+      EDK_FF(BK_TRANS_RANK)
       EDK_FF(BK_TRANS)
       EDK_FF(BK_TRANSPAR)
       default:

@@ -361,10 +361,17 @@ __global__ void k_rank_map(BasisDev b, int K, uint64_t n, uint32_t* out) {
       rem -= sb[p * 33 + j];
       --p;
     }
-    const uint32_t key =
-        b.runs_canon ? canon_runs32(s, b.L, mask) : canon_min32(s, b.L, b.A, b.len, mask);
+    uint32_t key;
+    int M = 0;
+    if (b.bk == BK_TRANS) key = canon_arg32(s, b.L, b.A, b.len, mask, M);
+    else key = b.runs_canon ? canon_runs32(s, b.L, mask) : canon_min32(s, b.L, b.A, b.len, mask);
     uint32_t v;
-    out[r] = hash_find(b, key, v) ? v : ~0u;
+    if (!hash_find(b, key, v)) {
+      out[r] = ~0u;
+      continue;
+    }
+    const uint32_t row = b.packed ? v >> 5 : v, cls = b.packed ? v & 31u : 0u;
+    out[r] = (row << b.rank_shift) | (b.rank_shift == 10 ? (uint32_t)M << 5 : 0u) | cls;
   }
 }
 
@@ -933,6 +940,7 @@ edk_status build_rank_table(edk_basis* b) {
   BasisDev tmp = b->dev;
   tmp.search = 0;
   tmp.binom32 = b->binom32.as<uint32_t>();
+  tmp.rank_shift = b->dev.rank_shift;
   k_rank_map<<<grid_for((int64_t)n), 256, 0, st>>>(tmp, K, n, b->rankmap.as<uint32_t>());
   EDK_TRY_CUDA(cudaGetLastError());
   EDK_RETURN_IF(b->rowrank.alloc(b->D * sizeof(uint32_t)));
@@ -961,11 +969,17 @@ extern "C" edk_status edk_basis_set_search(edk_basis* b, int32_t strategy) {
     return EDK_OK;
   }
   if (strategy == EDK_SEARCH_RANK) {
-    if (bk != BK_TRANS0 || b->L > 32) {
-      set_error("edk_basis_set_search: the rank table serves phase-free translation sectors "
-                "(TranslationalBasis k = 0) with L <= 32");
+    // entries: row << 10 | M << 5 | class while rows fit 22 bits, else (k = 0
+    // only, no phase needed) row << 5 | class
+    const int shift = b->D < (1ll << 22) ? 10 : 5;
+    if ((bk != BK_TRANS0 && bk != BK_TRANS) || b->L > 32 || (bk == BK_TRANS && shift != 10) ||
+        b->D >= (1ll << 27)) {
+      set_error("edk_basis_set_search: the rank table serves translation sectors "
+                "(TranslationalBasis) of fixed N with L <= 32, and fewer than 2^22 rows "
+                "when k has a phase");
       return EDK_UNSUPPORTED;
     }
+    b->dev.rank_shift = shift;
     EDK_RETURN_IF(build_rank_table(b));
     b->dev.rankmap = b->rankmap.as<uint32_t>();
     b->dev.binom32 = b->binom32.as<uint32_t>();
@@ -1047,8 +1061,9 @@ edk_status check_basis_dev(const BasisDev& b) {
   if (ok && b.search == 1 && b.packed && b.bk != BK_TENSOR && b.bk != BK_PROJ_RANK)
     ok = b.rcls8 != nullptr;
   if (ok && b.search == 2)
-    ok = b.bk == BK_TRANS0 && b.L <= 32 && b.rankmap != nullptr && b.binom32 != nullptr &&
-         b.rowrank != nullptr;
+    ok = (b.bk == BK_TRANS0 || (b.bk == BK_TRANS && b.rank_shift == 10)) && b.L <= 32 &&
+         b.rankmap != nullptr && b.binom32 != nullptr && b.rowrank != nullptr &&
+         (b.rank_shift == 5 || b.rank_shift == 10);
   if (b.D > 0 && !ok) {
     set_error("internal: basis tables missing for its lookup kind");
     return EDK_INVALID_ARG;

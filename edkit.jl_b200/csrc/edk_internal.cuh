@@ -127,7 +127,9 @@ enum LookupKind : int {
   BK_ABELIAN = 6,    // generic odometer over commuting generators
   // BK_TRANS0 basis searched through its rank table (EDK_SEARCH_RANK); only
   // the bond-family fast path instantiates it, every other path keeps the hash
-  BK_TRANS0_RANK = 7
+  BK_TRANS0_RANK = 7,
+  // BK_TRANS basis searched through its rank table (entries carry the shift M)
+  BK_TRANS_RANK = 8
 };
 
 constexpr int kMaxGen = 8;
@@ -170,9 +172,11 @@ struct BasisDev {
   int64_t nfence;
   const uint8_t* rcls8;    // norm class of each row (packed values), else null
   // rank table (edk_basis_set_search(EDK_SEARCH_RANK), search == 2): for every
-  // state with the sector's popcount, indexed by its colex rank, the hash value
-  // of its representative (row << 5 | class, or row) or ~0u when the orbit is
-  // not in the basis; binom32[p * 33 + k] = C(p, k) for p < 32
+  // state with the sector's popcount, indexed by its colex rank, the entry
+  // row << rank_shift | M << 5 | norm class of its representative (M, the
+  // first-minimum shift, only when rank_shift == 10), or ~0u when the orbit
+  // is not in the basis; binom32[p * 33 + k] = C(p, k) for p < 32
+  int rank_shift;            // 5 (row < 2^27, no M) or 10 (row < 2^22, with M)
   const uint32_t* rankmap;
   const uint32_t* binom32;
   const uint32_t* rowrank;   // colex rank of each representative I[i]

@@ -138,6 +138,14 @@ __device__ __forceinline__ void decode_val(const BasisDev& b, uint32_t v, int64_
   }
 }
 
+// decode a rank-table entry into (row, norm, first-minimum shift M)
+__device__ __forceinline__ void rank_decode(const BasisDev& b, uint32_t v, int64_t& pos,
+                                            double& rpos, int& M) {
+  pos = (int64_t)(v >> b.rank_shift);
+  M = (int)((v >> 5) & 31u);
+  rpos = b.packed ? b.Rcls[v & 31u] : __ldg(b.R + pos);
+}
+
 // colex rank of a fixed-popcount state (= its position among all states with
 // that popcount in ascending order); binom[p*33 + k] = C(p, k), p < 32.
 __device__ __forceinline__ int64_t colex_rank(uint32_t s, const uint32_t* binom) {

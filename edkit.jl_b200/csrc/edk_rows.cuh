@@ -282,10 +282,12 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
                                         VT* __restrict__ yk, int accumulate) {
   using A = typename VTraits<VT>::A;
   constexpr bool CX = VTraits<VT>::cx;
-  // BK_TRANS0_RANK: a phase-free translation sector whose target rows come
-  // from the rank table instead of canonicalisation + hash probe
-  constexpr bool RANKED = BK == BK_TRANS0_RANK;
-  constexpr int BKL = RANKED ? (int)BK_TRANS0 : BK;
+  // BK_TRANS0_RANK / BK_TRANS_RANK: a translation sector whose target rows
+  // (and, with a momentum phase, shifts M) come from the rank table instead of
+  // canonicalisation + hash probe
+  constexpr bool PHASED = BK == BK_TRANS_RANK;
+  constexpr bool RANKED = BK == BK_TRANS0_RANK || PHASED;
+  constexpr int BKL = BK == BK_TRANS0_RANK ? (int)BK_TRANS0 : (PHASED ? (int)BK_TRANS : BK);
   __shared__ uint32_t s_binom[(BK == BK_PROJ_RANK || RANKED) ? 32 * 33 : 1];
   __shared__ int s_hist[64];
   __shared__ unsigned short s_order[256];
@@ -394,8 +396,13 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
         ok2 = v2 != ~0u;
         pos1 = pos2 = 0;
         rp1 = rp2 = 1.0;
-        if (ok1) decode_val(b, v1, pos1, rp1);
-        if (ok2) decode_val(b, v2, pos2, rp2);
+        int M1 = 0, M2 = 0;
+        if (ok1) rank_decode(b, v1, pos1, rp1, M1);
+        if (ok2) rank_decode(b, v2, pos2, rp2, M2);
+        if constexpr (PHASED) {  // phase C[M] of the target, as index() gives it
+          if (ok1) { const double2 c = __ldg(b.phase + M1); h1.pre = c.x; h1.pim = c.y; }
+          if (ok2) { const double2 c = __ldg(b.phase + M2); h2.pre = c.x; h2.pim = c.y; }
+        }
       } else {
         const uint32_t s1 = st ^ (1u << p1) ^ (1u << q1), s2 = st ^ (1u << p2) ^ (1u << q2);
         canon_ctx<BKL>(b, s1, h1);

@@ -1,6 +1,7 @@
-"""The rank-table index search (EDK_SEARCH_RANK) of phase-free translation
-sectors: the bond-family row kernel finds target rows by updating the colex
-rank of the row state and reading one table entry.  Rows are the ones EDKit's
+"""The rank-table index search (EDK_SEARCH_RANK) of translation sectors of
+fixed N: the bond-family row kernel finds target rows (and, for k != 0, the
+shift that sets the phase) by updating the colex rank of the row state and
+reading one table entry.  Rows are the ones EDKit's
 index() gives, so H*x must equal the hash-table result bit for bit and the
 oracle's mul within 1e-12 (FP64)."""
 import numpy as np
@@ -72,7 +73,7 @@ def test_rank_search_with_predicate_and_unit_cell_rejected(ek, O):
     b.set_search("rank")
     H.configure_("fast", 1)
     assert rel(H * x, Ho.mul(x).real) < 1e-12
-    for bad in (ek.TranslationalBasis(L=L, k=1, N=7), ek.TranslationalBasis(L=L, k=0),
+    for bad in (ek.TranslationalBasis(L=L, k=1), ek.TranslationalBasis(L=L, k=0),
                 ek.TranslationParityBasis(L=L, k=0, p=1, N=7)):
         with pytest.raises(ek.EDKError):
             bad.set_search("rank")
@@ -147,3 +148,49 @@ def test_block_lanczos_mixes_ranked_and_phased_sectors(ek, O):
     ev, _ = ek.block_lanczos(ops, block=8, m=24, nev=3, check_every=0)
     for q in range(3):
         assert np.allclose(ev[q][:3], refs[q], rtol=0, atol=1e-9 * abs(refs[q][0])), q
+
+
+@pytest.mark.parametrize("L,N,k,a", [(12, 6, 1, 1), (16, 8, 3, 1), (16, 7, 8, 1), (20, 10, 7, 1),
+                                     (16, 8, 3, 2)])
+def test_rank_search_phased_sectors_bit_exact(ek, O, L, N, k, a):
+    """k != 0: the table entry also carries the first-minimum shift M, so the
+    phase C[M] equals the one index() gives; H*x bit-identical to the hash path."""
+    rng = np.random.default_rng(L * 100 + k)
+    b = ek.TranslationalBasis(L=L, k=k, N=N, a=a)
+    ops = [("xxz", ek.trans_inv_operator(ek.spin(*XXZ), 2, b))]
+    if a == 1:
+        ops.append(("j1j2+h", j1j2(ek, L, b, h=0.3)))
+    D = b.size(1)
+    for name, H in ops:
+        for dt in (np.complex128, np.complex64):
+            x = (rng.standard_normal(D) + 1j * rng.standard_normal(D)).astype(dt)
+            for tps in (1, 2):
+                H.configure_("fast", tps)
+                b.set_search("hash")
+                y_hash = H * x
+                b.set_search("rank")
+                y_rank = H * x
+                assert np.array_equal(y_rank, y_hash), (name, dt, tps)
+    o = O.translational(L, k=k, N=N, a=a)
+    Ho = O.trans_inv_operator(O.spin(*XXZ), 2, o)
+    x = rng.standard_normal(D) + 1j * rng.standard_normal(D)
+    b.set_search("rank")
+    ops[0][1].configure_("fast", 1)
+    assert rel(ops[0][1] * x, Ho.mul(x)) < 1e-12
+
+
+def test_rank_search_all_momentum_sectors_batched(ek, O):
+    """Every momentum sector rank-searched, one batched Lanczos (FP64 and
+    mixed) against the sectors' dense spectra."""
+    L = 14
+    ops, refs = [], []
+    for k in range(L):
+        b = ek.TranslationalBasis(L=L, k=k, N=7)
+        b.set_search("rank")
+        ops.append(ek.trans_inv_operator(ek.spin(*XXZ), 2, b))
+        Ho = O.trans_inv_operator(O.spin(*XXZ), 2, O.translational(L, k=k, N=7))
+        refs.append(np.linalg.eigvalsh(Ho.dense())[:2])
+    for prec in ("fp64", "mixed"):
+        ev, _ = ek.batch_lanczos_e0(ops, m=150, nev=2, tol=1e-12, check_every=5, precision=prec)
+        for q in range(L):
+            assert np.allclose(ev[q], refs[q], rtol=0, atol=1e-9 * abs(refs[q][0])), (prec, q)
