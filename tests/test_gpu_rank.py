@@ -194,3 +194,23 @@ def test_rank_search_all_momentum_sectors_batched(ek, O):
         ev, _ = ek.batch_lanczos_e0(ops, m=150, nev=2, tol=1e-12, check_every=5, precision=prec)
         for q in range(L):
             assert np.allclose(ev[q], refs[q], rtol=0, atol=1e-9 * abs(refs[q][0])), (prec, q)
+
+
+def test_run_canonicalisation_gives_the_same_rows(ek, monkeypatch):
+    """EDK_CANON_RUNS=1 canonicalises k = 0 states by comparing only the
+    rotations that start at a domain wall; the representative, hence every
+    row and H*x (hash and rank searches), is the same as the full scan's."""
+    L = 16
+    rng = np.random.default_rng(11)
+    b0 = ek.TranslationalBasis(L=L, k=0, N=8)
+    H0 = ek.trans_inv_operator(ek.spin(*XXZ), 2, b0)
+    x = rng.standard_normal(b0.size(1))
+    y0 = H0 * x
+    monkeypatch.setenv("EDK_CANON_RUNS", "1")
+    b1 = ek.TranslationalBasis(L=L, k=0, N=8)
+    monkeypatch.delenv("EDK_CANON_RUNS")
+    H1 = ek.trans_inv_operator(ek.spin(*XXZ), 2, b1)
+    assert np.array_equal(b1.I, b0.I) and np.array_equal(b1.R, b0.R)
+    assert np.array_equal(H1 * x, y0)
+    b1.set_search("rank")
+    assert np.array_equal(H1 * x, y0)
