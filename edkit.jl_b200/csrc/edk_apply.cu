@@ -50,12 +50,13 @@ __global__ void __launch_bounds__(256) k_apply(BasisDev b, OpDev op, const VT* _
 // Resident blocks per SM asked of the compiler: the rank-search kernels are
 // latency bound and fit 32 registers (8 blocks of 256 threads fill every warp
 // slot) for real and single-precision complex vectors, or single precision
-// when the sector has a phase; the others keep the compiler's choice.
+// when the sector has a phase or a parity; the others keep the compiler's
+// choice.
 template <int BK, class VT>
 constexpr int ff_min_blocks() {
+  constexpr bool single = std::is_same<VT, float>::value || std::is_same<VT, float2>::value;
   return (BK == BK_TRANS0_RANK && !std::is_same<VT, double2>::value) ||
-                 (BK == BK_TRANS_RANK && (std::is_same<VT, float>::value ||
-                                          std::is_same<VT, float2>::value))
+                 ((BK == BK_TRANS_RANK || BK == BK_TRANSPAR_RANK) && single)
              ? 8 : 1;
 }
 
@@ -100,7 +101,8 @@ edk_status launch_apply_ff(const BasisDev& b, const OpDev& op, const FFParams& f
     break;
     const int kind = b.search != 2 ? b.bk
                      : (b.bk == BK_TRANS0 ? (int)BK_TRANS0_RANK
-                                          : (b.bk == BK_TRANS ? (int)BK_TRANS_RANK : b.bk));
+                        : (b.bk == BK_TRANS ? (int)BK_TRANS_RANK
+                           : (b.bk == BK_TRANSPAR ? (int)BK_TRANSPAR_RANK : b.bk)));
     switch (kind) {
       EDK_FF(BK_TENSOR)
       EDK_FF(BK_PROJ_RANK)
@@ -108,6 +110,7 @@ edk_status launch_apply_ff(const BasisDev& b, const OpDev& op, const FFParams& f
       EDK_FF(BK_TRANS0)
       EDK_FF(BK_TRANS0_RANK)
       EDK_FF(BK_TRANS_RANK)
+      EDK_FF(BK_TRANSPAR_RANK)
       EDK_FF(BK_TRANS)
       EDK_FF(BK_TRANSPAR)
       default:

@@ -361,17 +361,29 @@ __global__ void k_rank_map(BasisDev b, int K, uint64_t n, uint32_t* out) {
       rem -= sb[p * 33 + j];
       --p;
     }
-    uint32_t key;
-    int M = 0;
-    if (b.bk == BK_TRANS) key = canon_arg32(s, b.L, b.A, b.len, mask, M);
-    else key = b.runs_canon ? canon_runs32(s, b.L, mask) : canon_min32(s, b.L, b.A, b.len, mask);
+    uint32_t key, extra = 0;  // extra: M (BK_TRANS) or the sign bit (BK_TRANSPAR)
+    if (b.bk == BK_TRANS) {
+      int M = 0;
+      key = canon_arg32(s, b.L, b.A, b.len, mask, M);
+      extra = (uint32_t)M;
+    } else if (b.bk == BK_TRANSPAR) {  // the coefficient rule of lookup<BK_TRANSPAR>
+      uint32_t Iam, Ibm;
+      int Rr, M;
+      canon_par32(s, b.L, b.A, b.len, mask, Iam, Rr, Ibm, M);
+      double n;
+      if (Ibm < Iam) { key = Ibm; n = (double)b.P * __ldg(b.phase + M).x; }
+      else { key = Iam; n = __ldg(b.phase + Rr).x; }
+      extra = n < 0.0 ? 1u : 0u;
+    } else {
+      key = b.runs_canon ? canon_runs32(s, b.L, mask) : canon_min32(s, b.L, b.A, b.len, mask);
+    }
     uint32_t v;
     if (!hash_find(b, key, v)) {
       out[r] = ~0u;
       continue;
     }
     const uint32_t row = b.packed ? v >> 5 : v, cls = b.packed ? v & 31u : 0u;
-    out[r] = (row << b.rank_shift) | (b.rank_shift == 10 ? (uint32_t)M << 5 : 0u) | cls;
+    out[r] = (row << b.rank_shift) | (b.rank_shift > 5 ? extra << 5 : 0u) | cls;
   }
 }
 
@@ -971,12 +983,12 @@ extern "C" edk_status edk_basis_set_search(edk_basis* b, int32_t strategy) {
   if (strategy == EDK_SEARCH_RANK) {
     // entries: row << 10 | M << 5 | class while rows fit 22 bits, else (k = 0
     // only, no phase needed) row << 5 | class
-    const int shift = b->D < (1ll << 22) ? 10 : 5;
-    if ((bk != BK_TRANS0 && bk != BK_TRANS) || b->L > 32 || (bk == BK_TRANS && shift != 10) ||
-        b->D >= (1ll << 27)) {
-      set_error("edk_basis_set_search: the rank table serves translation sectors "
-                "(TranslationalBasis) of fixed N with L <= 32, and fewer than 2^22 rows "
-                "when k has a phase");
+    const int shift = bk == BK_TRANSPAR ? 6 : (b->D < (1ll << 22) ? 10 : 5);
+    if ((bk != BK_TRANS0 && bk != BK_TRANS && bk != BK_TRANSPAR) || b->L > 32 ||
+        (bk == BK_TRANS && shift != 10) || b->D >= (1ll << (32 - shift))) {
+      set_error("edk_basis_set_search: the rank table serves translation and "
+                "translation-parity sectors of fixed N with L <= 32 (fewer than 2^22 rows "
+                "when k has a phase, 2^26 with parity)");
       return EDK_UNSUPPORTED;
     }
     b->dev.rank_shift = shift;
@@ -1061,9 +1073,10 @@ edk_status check_basis_dev(const BasisDev& b) {
   if (ok && b.search == 1 && b.packed && b.bk != BK_TENSOR && b.bk != BK_PROJ_RANK)
     ok = b.rcls8 != nullptr;
   if (ok && b.search == 2)
-    ok = (b.bk == BK_TRANS0 || (b.bk == BK_TRANS && b.rank_shift == 10)) && b.L <= 32 &&
-         b.rankmap != nullptr && b.binom32 != nullptr && b.rowrank != nullptr &&
-         (b.rank_shift == 5 || b.rank_shift == 10);
+    ok = ((b.bk == BK_TRANS0 && (b.rank_shift == 5 || b.rank_shift == 10)) ||
+          (b.bk == BK_TRANS && b.rank_shift == 10) ||
+          (b.bk == BK_TRANSPAR && b.rank_shift == 6)) &&
+         b.L <= 32 && b.rankmap != nullptr && b.binom32 != nullptr && b.rowrank != nullptr;
   if (b.D > 0 && !ok) {
     set_error("internal: basis tables missing for its lookup kind");
     return EDK_INVALID_ARG;

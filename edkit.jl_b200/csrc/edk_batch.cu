@@ -543,6 +543,10 @@ struct BatchEngine {
           k_bapply_ff<BK_TRANS_RANK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv,
                                                                           stp, dn);
           break;
+        case BK_TRANSPAR_RANK:
+          k_bapply_ff<BK_TRANSPAR_RANK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv,
+                                                                             wv, stp, dn);
+          break;
         EDK_BAPPLY(BK_TRANS)
         EDK_BAPPLY(BK_TRANSPAR)
         default:
@@ -812,10 +816,11 @@ edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczo
   }
   // translation sectors searched through their rank tables (with a phase:
   // every table must carry the shift M)
-  bool ranked = (bk == BK_TRANS0 || bk == BK_TRANS) && ff;
+  bool ranked = (bk == BK_TRANS0 || bk == BK_TRANS || bk == BK_TRANSPAR) && ff;
   for (auto* op : ops)
-    ranked = ranked && op->b->dev.search == 2 && (bk == BK_TRANS0 || op->b->dev.rank_shift == 10);
-  if (ranked) bk = bk == BK_TRANS0 ? BK_TRANS0_RANK : BK_TRANS_RANK;
+    ranked = ranked && op->b->dev.search == 2 && (bk != BK_TRANS || op->b->dev.rank_shift == 10);
+  if (ranked)
+    bk = bk == BK_TRANS0 ? BK_TRANS0_RANK : (bk == BK_TRANS ? BK_TRANS_RANK : BK_TRANSPAR_RANK);
   if (bk == BK_ABELIAN && !all_mat) {
     set_error("batch Lanczos: symmetry-group (abelian) bases run one at a time unless materialised");
     return EDK_UNSUPPORTED;

@@ -129,7 +129,9 @@ enum LookupKind : int {
   // the bond-family fast path instantiates it, every other path keeps the hash
   BK_TRANS0_RANK = 7,
   // BK_TRANS basis searched through its rank table (entries carry the shift M)
-  BK_TRANS_RANK = 8
+  BK_TRANS_RANK = 8,
+  // BK_TRANSPAR basis searched through its rank table (entries carry the sign)
+  BK_TRANSPAR_RANK = 9
 };
 
 constexpr int kMaxGen = 8;
@@ -174,9 +176,10 @@ struct BasisDev {
   // rank table (edk_basis_set_search(EDK_SEARCH_RANK), search == 2): for every
   // state with the sector's popcount, indexed by its colex rank, the entry
   // row << rank_shift | M << 5 | norm class of its representative (M, the
-  // first-minimum shift, only when rank_shift == 10), or ~0u when the orbit
-  // is not in the basis; binom32[p * 33 + k] = C(p, k) for p < 32
-  int rank_shift;            // 5 (row < 2^27, no M) or 10 (row < 2^22, with M)
+  // first-minimum shift, only when rank_shift == 10; for translation + parity
+  // sectors rank_shift == 6 and bit 5 is the sign of the coefficient), or ~0u
+  // when the orbit is not in the basis; binom32[p * 33 + k] = C(p, k), p < 32
+  int rank_shift;            // 5 (row < 2^27), 6 (row < 2^26, sign), 10 (row < 2^22, M)
   const uint32_t* rankmap;
   const uint32_t* binom32;
   const uint32_t* rowrank;   // colex rank of each representative I[i]

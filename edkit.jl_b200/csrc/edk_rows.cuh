@@ -286,8 +286,10 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
   // (and, with a momentum phase, shifts M) come from the rank table instead of
   // canonicalisation + hash probe
   constexpr bool PHASED = BK == BK_TRANS_RANK;
-  constexpr bool RANKED = BK == BK_TRANS0_RANK || PHASED;
-  constexpr int BKL = BK == BK_TRANS0_RANK ? (int)BK_TRANS0 : (PHASED ? (int)BK_TRANS : BK);
+  constexpr bool SIGNED = BK == BK_TRANSPAR_RANK;  // translation + parity: coefficient +-1
+  constexpr bool RANKED = BK == BK_TRANS0_RANK || PHASED || SIGNED;
+  constexpr int BKL = BK == BK_TRANS0_RANK ? (int)BK_TRANS0
+                      : (PHASED ? (int)BK_TRANS : (SIGNED ? (int)BK_TRANSPAR : BK));
   __shared__ uint32_t s_binom[(BK == BK_PROJ_RANK || RANKED) ? 32 * 33 : 1];
   __shared__ int s_hist[64];
   __shared__ unsigned short s_order[256];
@@ -402,6 +404,10 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
         if constexpr (PHASED) {  // phase C[M] of the target, as index() gives it
           if (ok1) { const double2 c = __ldg(b.phase + M1); h1.pre = c.x; h1.pim = c.y; }
           if (ok2) { const double2 c = __ldg(b.phase + M2); h2.pre = c.x; h2.pim = c.y; }
+        }
+        if constexpr (SIGNED) {  // bit 5 of the entry: the coefficient is -1
+          h1.pre = ((v1 >> 5) & 1u) ? -1.0 : 1.0;
+          h2.pre = ((v2 >> 5) & 1u) ? -1.0 : 1.0;
         }
       } else {
         const uint32_t s1 = st ^ (1u << p1) ^ (1u << q1), s2 = st ^ (1u << p2) ^ (1u << q2);

@@ -128,7 +128,8 @@ extern "C" edk_status edk_operator_autotune(edk_operator* op, int32_t dtype, int
   // the rank table (4 bytes per state of the charge sector) when it applies
   // and takes at most a quarter of the free memory
   if (has_search && op->ff_ok && op->gather && b->L <= 32 &&
-      (b->dev.bk == BK_TRANS0 || (b->dev.bk == BK_TRANS && b->D < (1ll << 22)))) {
+      (b->dev.bk == BK_TRANS0 || (b->dev.bk == BK_TRANS && b->D < (1ll << 22)) ||
+       (b->dev.bk == BK_TRANSPAR && b->D < (1ll << 26)))) {
     size_t freeb = 0, totalb = 0;
     if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess &&
         (b->rankmap.p || rank_table_bytes(b) <= freeb / 4) &&

@@ -141,15 +141,16 @@ edk_status edk_basis_index_noalloc(const edk_basis* b, int64_t n, const uint64_t
  * strictly ascending. */
 #define EDK_SEARCH_HASH 0
 #define EDK_SEARCH_SORTED 1
-/* EDK_SEARCH_RANK: translation sectors (TranslationalBasis) of fixed N with
- * L <= 32; with a momentum phase (k != 0 and not absorbed) the sector must
- * have fewer than 2^22 rows.  A table over every state of the charge sector,
- * indexed by the state's colex rank, holds the row of its orbit
- * representative and the first-minimum shift M that sets its phase
- * (4 * C(L, N) bytes: 160 MB at L = 28, 2.4 GB at L = 32); the bond-family
- * row kernel then finds a target row by updating the row state's rank for
- * the exchanged pair of sites and reading one table entry, with no
- * canonicalisation.  Rows and phases are identical to the other strategies'.
+/* EDK_SEARCH_RANK: translation and translation-parity sectors
+ * (TranslationalBasis, TranslationParityBasis) of fixed N with L <= 32; with a
+ * momentum phase the sector must have fewer than 2^22 rows, with parity fewer
+ * than 2^26.  A table over every state of the charge sector, indexed by the
+ * state's colex rank, holds the row of its orbit representative and the
+ * first-minimum shift M that sets its phase (for translation-parity sectors,
+ * the sign of the coefficient); 4 * C(L, N) bytes: 160 MB at L = 28, 2.4 GB
+ * at L = 32.  The bond-family row kernel then finds a target row by updating
+ * the row state's rank for the exchanged pair of sites and reading one table
+ * entry, with no canonicalisation.  Rows and phases are identical to the other strategies'.
  * Paths other than the bond-family row kernel keep using the hash table. */
 #define EDK_SEARCH_RANK 2
 edk_status edk_basis_set_search(edk_basis* b, int32_t strategy);

@@ -74,7 +74,7 @@ def test_rank_search_with_predicate_and_unit_cell_rejected(ek, O):
     H.configure_("fast", 1)
     assert rel(H * x, Ho.mul(x).real) < 1e-12
     for bad in (ek.TranslationalBasis(L=L, k=1), ek.TranslationalBasis(L=L, k=0),
-                ek.TranslationParityBasis(L=L, k=0, p=1, N=7)):
+                ek.TranslationParityBasis(L=L, k=0, p=1), ek.ProjectedBasis(L=L, N=7, f=pxp)):
         with pytest.raises(ek.EDKError):
             bad.set_search("rank")
 
@@ -214,3 +214,45 @@ def test_run_canonicalisation_gives_the_same_rows(ek, monkeypatch):
     assert np.array_equal(H1 * x, y0)
     b1.set_search("rank")
     assert np.array_equal(H1 * x, y0)
+
+
+@pytest.mark.parametrize("L,N,k,p", [(12, 6, 0, 1), (14, 7, 0, -1), (16, 8, 8, 1), (16, 7, 8, -1),
+                                     (20, 10, 0, 1)])
+def test_rank_search_translation_parity_bit_exact(ek, O, L, N, k, p):
+    """TranslationParityBasis: the entry carries the sign of the coefficient
+    (P C[M] or C[R], +-1), so H*x is bit-identical to the hash path."""
+    rng = np.random.default_rng(L * 10 + N + k)
+    b = ek.TranslationParityBasis(L=L, k=k, p=p, N=N)
+    ops = [("xxz", ek.trans_inv_operator(ek.spin(*XXZ), 2, b)), ("j1j2+h", j1j2(ek, L, b, h=0.3))]
+    D = b.size(1)
+    for name, H in ops:
+        for dt in (np.float64, np.float32, np.complex128):
+            x = rng.standard_normal(D).astype(dt)
+            if np.iscomplexobj(x):
+                x = x + 1j * rng.standard_normal(D)
+            for tps in (1, 2):
+                H.configure_("fast", tps)
+                b.set_search("hash")
+                y_hash = H * x
+                b.set_search("rank")
+                assert np.array_equal(H * x, y_hash), (name, dt, tps)
+    if L <= 16:
+        o = O.transparity(L, k=k, p=p, N=N)
+        Ho = O.trans_inv_operator(O.spin(*XXZ), 2, o)
+        x = rng.standard_normal(D)
+        b.set_search("rank")
+        ops[0][1].configure_("fast", 1)
+        assert rel(ops[0][1] * x, Ho.mul(x).real) < 1e-12
+    # batched Lanczos over both parities, rank-searched
+    ops2, refs = [], []
+    if L <= 14:
+        for pp in (1, -1):
+            bb = ek.TranslationParityBasis(L=L, k=k, p=pp, N=N)
+            bb.set_search("rank")
+            ops2.append(ek.trans_inv_operator(ek.spin(*XXZ), 2, bb))
+            Ho = O.trans_inv_operator(O.spin(*XXZ), 2, O.transparity(L, k=k, p=pp, N=N))
+            refs.append(np.linalg.eigvalsh(Ho.dense())[0])
+        ev, _ = ek.batch_lanczos_e0(ops2, m=min(120, min(o.size(1) for o in ops2) - 1), nev=1,
+                                    tol=1e-13, check_every=5)
+        for q in range(2):
+            assert abs(ev[q][0] - refs[q]) <= 1e-10 * abs(refs[q]), q
