@@ -131,7 +131,6 @@ __global__ void __launch_bounds__(256) k_spmm_ff(const SpmmOp* __restrict__ ops,
     fill_binom32(s_binom);
     __syncthreads();
   }
-  const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t total = (int64_t)nops * Dpad;
@@ -218,7 +217,6 @@ __global__ void __launch_bounds__(256) k_spmm_sell(const SpmmOp* __restrict__ op
                                                    const VT* __restrict__ X, VT* __restrict__ Y,
                                                    int accumulate) {
   using A = typename VTraits<VT>::A;
-  const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t total = (int64_t)nops * smax;
