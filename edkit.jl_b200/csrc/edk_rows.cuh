@@ -339,8 +339,12 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
   if (TPS == 1 && !valid) return;
   const uint32_t st = s_state[tt];  // 0 past the last row: no hits
   const A invRi = (b.R && valid) ? (A)(1.0 / __ldg(b.R + i)) : (A)1;
+  // complete fixed-charge sector (BK_PROJ_RANK): a state's row is its colex
+  // rank, so target rows follow from the row index by the same rank update
+  constexpr bool DIRECT = BK == BK_PROJ_RANK;
   uint32_t rs = 0;  // colex rank of the row state (rank-table search)
   if constexpr (RANKED) rs = valid ? __ldg(b.rowrank + i) : 0u;
+  if constexpr (DIRECT) rs = (uint32_t)i;
   int pc = 0;  // pairs of hits seen so far in this row
   double dr = 0.0, di = 0.0;
   A ar = 0, ai = 0;
@@ -377,7 +381,7 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
       int64_t pos1, pos2;
       double rp1, rp2;
       bool ok1, ok2;
-      if constexpr (RANKED) {
+      if constexpr (RANKED || DIRECT) {
         h1 = h2 = HitCtx{0u, 1.0, 0.0};
         uint32_t k1, k2;
         if (d == 1 && p1 != 0) {
@@ -392,22 +396,30 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
           k1 = rank_after_swap(st, rs, p1, q1, s_binom);
           k2 = two ? rank_after_swap(st, rs, p2, q2, s_binom) : k1;
         }
-        const uint32_t v1 = __ldg(b.rankmap + k1);
-        const uint32_t v2 = two ? __ldg(b.rankmap + k2) : ~0u;
-        ok1 = v1 != ~0u;
-        ok2 = v2 != ~0u;
-        pos1 = pos2 = 0;
-        rp1 = rp2 = 1.0;
-        int M1 = 0, M2 = 0;
-        if (ok1) rank_decode(b, v1, pos1, rp1, M1);
-        if (ok2) rank_decode(b, v2, pos2, rp2, M2);
-        if constexpr (PHASED) {  // phase C[M] of the target, as index() gives it
-          if (ok1) { const double2 c = __ldg(b.phase + M1); h1.pre = c.x; h1.pim = c.y; }
-          if (ok2) { const double2 c = __ldg(b.phase + M2); h2.pre = c.x; h2.pim = c.y; }
-        }
-        if constexpr (SIGNED) {  // bit 5 of the entry: the coefficient is -1
-          h1.pre = ((v1 >> 5) & 1u) ? -1.0 : 1.0;
-          h2.pre = ((v2 >> 5) & 1u) ? -1.0 : 1.0;
+        if constexpr (DIRECT) {  // the exchange keeps the charge: both targets are rows
+          pos1 = (int64_t)k1;
+          pos2 = (int64_t)k2;
+          rp1 = rp2 = 1.0;
+          ok1 = true;
+          ok2 = two;
+        } else {
+          const uint32_t v1 = __ldg(b.rankmap + k1);
+          const uint32_t v2 = two ? __ldg(b.rankmap + k2) : ~0u;
+          ok1 = v1 != ~0u;
+          ok2 = v2 != ~0u;
+          pos1 = pos2 = 0;
+          rp1 = rp2 = 1.0;
+          int M1 = 0, M2 = 0;
+          if (ok1) rank_decode(b, v1, pos1, rp1, M1);
+          if (ok2) rank_decode(b, v2, pos2, rp2, M2);
+          if constexpr (PHASED) {  // phase C[M] of the target, as index() gives it
+            if (ok1) { const double2 c = __ldg(b.phase + M1); h1.pre = c.x; h1.pim = c.y; }
+            if (ok2) { const double2 c = __ldg(b.phase + M2); h2.pre = c.x; h2.pim = c.y; }
+          }
+          if constexpr (SIGNED) {  // bit 5 of the entry: the coefficient is -1
+            h1.pre = ((v1 >> 5) & 1u) ? -1.0 : 1.0;
+            h2.pre = ((v2 >> 5) & 1u) ? -1.0 : 1.0;
+          }
         }
       } else {
         const uint32_t s1 = st ^ (1u << p1) ^ (1u << q1), s2 = st ^ (1u << p2) ^ (1u << q2);
