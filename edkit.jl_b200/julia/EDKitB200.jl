@@ -22,6 +22,7 @@ import Base: *, size, eltype
 import LinearAlgebra: mul!
 
 export B200Operator, B200Basis, lanczos_e0, ground_state, timeevolve, autotune!, block_lanczos,
+       set_search!,
        schmidt_b200, ent_S_b200, double_basis_b200, symmetrizer_b200
 
 const libedk = get(ENV, "EDK_LIB", joinpath(@__DIR__, "..", "libedk.so"))
@@ -289,6 +290,21 @@ end
 timeevolve(H::B200Operator, ψ0::AbstractVector, t::Real; kw...) =
     (t < 0 && error("timeevolve!: requested time $t precedes anchor time 0.0");
      timeevolve(H, ψ0, [t]; kw...)[:, 1])
+
+"""
+    set_search!(H::B200Operator, strategy::Symbol)
+
+Index search of the operator's basis: `:hash` (default), `:sorted` (the
+binary search of EDKit's `index`) or `:rank` (translation and
+translation-parity sectors of fixed N: the rank table, the fastest
+matrix-free search).  Rows and results are the same for every choice.
+"""
+function set_search!(H::B200Operator, strategy::Symbol)
+    code = strategy === :hash ? 0 : strategy === :sorted ? 1 : strategy === :rank ? 2 :
+           error("unknown index search $strategy")
+    check(ccall((:edk_basis_set_search, libedk), Cint, (Ptr{Cvoid}, Int32), H.basis.h, code))
+    H
+end
 
 # --- eigenvector post-processing (src/Schmidt.jl, src/LinearMap.jl) ---
 _vdt(::AbstractVector{Float64}) = Int32(0)
