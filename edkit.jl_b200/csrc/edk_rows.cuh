@@ -350,14 +350,18 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
   A ar = 0, ai = 0;
   // bases whose index() coefficient has no phase (1 + 0i): the products with
   // the phase are skipped (equal values; only the sign of a zero may differ)
+  // (translation + parity: a real +-1 phase, the imaginary products are skipped)
   constexpr bool UNIT_PHASE =
       BKL == BK_TENSOR || BKL == BK_PROJ_RANK || BKL == BK_PROJ_HASH || BKL == BK_TRANS0;
+  constexpr bool REAL_PHASE = BKL == BK_TRANSPAR;
   auto acc = [&](const HitCtx& c, double rpos, double vr, double vi, Cx<A> xv) {
     const A pr = (A)c.pre, pi = (A)c.pim, v_r = (A)vr, v_i = (A)vi;
     const A ratio = (A)rpos * invRi;
-    const A cr = UNIT_PHASE ? v_r * ratio : (v_r * pr - v_i * pi) * ratio;
+    const A cr = UNIT_PHASE ? v_r * ratio
+                 : REAL_PHASE ? (v_r * pr) * ratio : (v_r * pr - v_i * pi) * ratio;
     if constexpr (CX) {
-      const A ci = UNIT_PHASE ? v_i * ratio : (v_r * pi + v_i * pr) * ratio;
+      const A ci = UNIT_PHASE ? v_i * ratio
+                   : REAL_PHASE ? (v_i * pr) * ratio : (v_r * pi + v_i * pr) * ratio;
       ar += cr * xv.r + ci * xv.i;
       ai += cr * xv.i - ci * xv.r;
     } else {
