@@ -295,6 +295,7 @@ edk_status apply_device(edk_operator* op, int dtype, const void* x, void* y, int
     return apply_block(op, dtype, x, y, nvec, ldx, ldy, accumulate, st);
   if (op->sell_ok && !sc) return apply_sell(op, dtype, x, y, nvec, ldx, ldy, accumulate, st);
   if (op->ff_ok && !sc && op->use_ff) {
+    if (plan_applies(op)) return apply_plan(op, dtype, x, y, nvec, ldx, ldy, accumulate, st, 0, -1);
     const FFParams& ff = *reinterpret_cast<const FFParams*>(op->ff_params.data());
 #define EDK_FF_TPS(VT)                                                                          \
   switch (op->tps) {                                                                            \
@@ -465,6 +466,7 @@ edk_status apply_rows(edk_operator* op, int dtype, const void* x, void* y, int64
   const BasisDev& b = op->b->dev;
   EDK_RETURN_IF(check_basis_dev(b));
   if (op->sell_ok) return apply_sell_rows(op, dtype, x, y, row0, row1, accumulate, st);
+  if (plan_applies(op)) return apply_plan(op, dtype, x, y, 1, b.D, b.D, accumulate, st, row0, row1);
   const FFParams& ff = *reinterpret_cast<const FFParams*>(op->ff_params.data());
   const int64_t D = b.D;
 #define EDK_FF_ROWS(VT)                                                                      \
@@ -561,6 +563,7 @@ extern "C" edk_status edk_operator_create(edk_basis* b, int32_t nterms, const in
   op->gather = herm;
   op->is_complex = cplx;
   if (const char* e = std::getenv("EDK_DISABLE_FAST")) op->use_ff = !(e[0] == '1');
+  if (const char* e = std::getenv("EDK_DISABLE_PLAN")) op->use_plan = !(e[0] == '1');
   // families of 2-site terms with one shared matrix
   std::map<std::pair<int, std::vector<double>>, std::vector<int>> groups;
   for (size_t t = 0; t < terms.size(); ++t) {
@@ -646,6 +649,7 @@ extern "C" edk_status edk_operator_create(edk_basis* b, int32_t nterms, const in
         for (int c = 0; c < 4; ++c) ff.dval[f][c] = fams[f].dval[c];
         ff.v1[f] = fams[f].val[1][0];
         ff.v2[f] = fams[f].val[2][0];
+        ff.same[f] = ff.v1[f].x == ff.v2[f].x && ff.v1[f].y == ff.v2[f].y;
       }
       op->ff_params.resize(sizeof(FFParams));
       std::memcpy(op->ff_params.data(), &ff, sizeof(FFParams));

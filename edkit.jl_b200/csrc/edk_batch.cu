@@ -28,7 +28,7 @@
 #include <memory>
 #include <vector>
 
-#include "edk_rows.cuh"
+#include "edk_rankrows.cuh"
 
 namespace edk {
 
@@ -93,6 +93,25 @@ __global__ void __launch_bounds__(256) k_bapply_ff(const BOp* __restrict__ ops,
   const int j = *step;
   ff_tile<BK, VT>(o.b, o.op, o.ff, (blockIdx.x - o.tile0) * (int64_t)kTile,
                   V + o.voff + (int64_t)j * o.D, wt + o.woff, 0);
+}
+
+// the row-plan form of k_bapply_ff (rank-searched sectors whose operators all
+// carry a plan): tile t of operator q is window t of q's plan
+template <int BK, class VT>
+__global__ void __launch_bounds__(256) k_bapply_plan(const BOp* __restrict__ ops,
+                                                     const int* __restrict__ tile2op,
+                                                     const VT* __restrict__ V, VT* __restrict__ wt,
+                                                     const int* __restrict__ step,
+                                                     const int* __restrict__ done) {
+  __shared__ FFTab<BK> sm;
+  const int q = tile2op[blockIdx.x];
+  if (done[q]) return;
+  const BOp& o = ops[q];
+  ff_tab_fill<BK>(sm, o.b, o.op.plan.binom);
+  __syncthreads();
+  const int j = *step;
+  plan_row<BK, VT>(o.b, o.op, o.ff, sm, (blockIdx.x - o.tile0) * (int64_t)kTile + threadIdx.x,
+                   V + o.voff + (int64_t)j * o.D, wt + o.woff, 0);
 }
 
 template <class VT>
@@ -296,8 +315,9 @@ __global__ void __launch_bounds__(256) k_bfinish(const BOp* __restrict__ ops, in
   double n2 = 0.0;
   for (int k = 0; k < 8; ++k) n2 += sh[k];
   const double nrm = sqrt(n2);
-  if (setup) {  // starting vector: zero norm is an error for this operator
-    if (!(nrm > 0.0)) { done[q] = 3; invb[q] = 0.0; }
+  if (setup) {  // starting vector: zero or non-finite norm is an error for this operator
+    if (!isfinite(nrm)) { done[q] = 4; invb[q] = 0.0; }
+    else if (!(nrm > 0.0)) { done[q] = 3; invb[q] = 0.0; }
     else invb[q] = 1.0 / nrm;
     return;
   }
@@ -385,6 +405,7 @@ struct BatchEngine {
   int nops = 0, vdt = EDK_F64, wdt = EDK_F64, ncap = 0, m = 0;
   int bk = 0;
   bool ff = false;
+  bool plan = false;  // every operator carries a row plan (rank-searched sectors)
   bool sell = false;
   int64_t nsblk = 0;
   cudaStream_t st = nullptr;
@@ -405,6 +426,15 @@ struct BatchEngine {
   edk_status init(const std::vector<edk_operator*>& ops, int vdtype, int m_, int lookup_kind,
                   bool use_ff, cudaStream_t s) {
     nops = (int)ops.size();
+    // row plans (built here, outside any capture) when the sectors are ranked
+    plan = use_ff && (lookup_kind == BK_TRANS0_RANK || lookup_kind == BK_TRANS_RANK ||
+                      lookup_kind == BK_TRANSPAR_RANK || lookup_kind == BK_PROJ_RANK);
+    for (auto* op : ops) {
+      if (!plan) break;
+      if (!plan_applies(op)) { plan = false; break; }
+      EDK_RETURN_IF(plan_ensure(op));
+      plan = op->plan_state == 1;
+    }
     vdt = vdtype;
     wdt = (vdt == EDK_C128 || vdt == EDK_C64) ? EDK_C128 : EDK_F64;
     m = m_;
@@ -524,6 +554,22 @@ struct BatchEngine {
           k_bapply_sell<VT><<<(unsigned)nsblk, 256, 0, st>>>(d_ops(), sblk2op.as<int>(), Vv, wv,
                                                              stp, dn);
         return EDK_OK;
+      }
+      if (plan) {
+        switch (bk) {
+          case BK_PROJ_RANK:
+            k_bapply_plan<BK_PROJ_RANK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+            return EDK_OK;
+          case BK_TRANS0_RANK:
+            k_bapply_plan<BK_TRANS0_RANK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+            return EDK_OK;
+          case BK_TRANS_RANK:
+            k_bapply_plan<BK_TRANS_RANK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+            return EDK_OK;
+          case BK_TRANSPAR_RANK:
+            k_bapply_plan<BK_TRANSPAR_RANK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+            return EDK_OK;
+        }
       }
 #define EDK_BAPPLY(BK)                                                                       \
   case BK:                                                                                   \
@@ -859,11 +905,16 @@ edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczo
   EDK_RETURN_IF(run_batch(E, o.max_steps, o.nev, tol1, check1, res, &nchecks));
   double ts2 = wall();
   int rounds = 0;
-  for (int q = 0; q < nops; ++q)
+  for (int q = 0; q < nops; ++q) {
+    if (res[q].status == 4) {
+      set_error("Initial state has non-finite entries (NaN or Inf)");
+      return EDK_INVALID_ARG;
+    }
     if (res[q].status == 3) {
       set_error("Initial state has zero norm");
       return EDK_ZERO_NORM;
     }
+  }
   int steps_low = 0, mvs = 0, bd = 0;
   for (auto& r : res) { steps_low = std::max(steps_low, r.steps); mvs += r.steps; bd |= r.status == 2; }
   // global element offset of each operator in the concatenated layout

@@ -73,6 +73,7 @@ struct DevBuf {
     if (n == 0) return EDK_OK;
     cudaError_t e = cudaMalloc(&p, n);
     if (e != cudaSuccess) {
+      cudaGetLastError();  // an allocation failure is not sticky: clear it for later checks
       p = nullptr;
       set_error(std::string("cudaMalloc(") + std::to_string(n) + " bytes) failed: " +
                 cudaGetErrorString(e));
@@ -103,6 +104,7 @@ inline edk_status DevBuf::alloc_async(size_t n, cudaStream_t s) {
   keep_pool_memory();
   cudaError_t e = cudaMallocAsync(&p, n, s);
   if (e != cudaSuccess) {
+    cudaGetLastError();  // an allocation failure is not sticky: clear it for later checks
     p = nullptr;
     set_error(std::string("cudaMallocAsync(") + std::to_string(n) + " bytes) failed: " +
               cudaGetErrorString(e));
@@ -225,6 +227,7 @@ struct FFParams {
   double2 dval[kMaxFF][4];
   double2 v1[kMaxFF];  // M[2][1]: local column "01" -> row "10"
   double2 v2[kMaxFF];  // M[1][2]: local column "10" -> row "01"
+  int same[kMaxFF];    // 1 when v1 == v2 (one accumulator for both directions)
 };
 
 // Materialised operator (the device counterpart of sparse!(opt)): sliced
@@ -252,8 +255,24 @@ struct SellDev {
   const float2* vt32;      // the same table rounded to FP32
 };
 
+constexpr int kPlanWindow = 256;  // rows per window of a row plan (and per thread block)
+// Device view of a row plan: slot k of window w describes row
+// rw[k] & kPlanRowMask of that window (rows sorted by their number of hits).
+struct RowPlanDev {
+  const uint32_t* st;     // row state (L <= 32)
+  const uint32_t* rk;     // colex rank of the row state (the row itself for complete sectors)
+  const uint32_t* rw;     // row | norm class << 27; ~0u pads the last window
+  const uint32_t* rkw;    // rank of the state with bits 0 and L-1 exchanged (the
+                          // wrap-around bond of a nearest-neighbour family), or ~0u
+  const double* dg;       // diagonal of the row (operators with diagonal-only generic terms), or null
+  const uint32_t* binom;  // binom[p * 33 + k] = C(p, k), p < 32
+  int64_t nslots;         // windows * 256
+};
+constexpr uint32_t kPlanRowMask = (1u << 27) - 1u;
+
 struct OpDev {
   SellDev sell;
+  RowPlanDev plan;          // row plan of the rank-searched fast path (plan.rw null: none)
   int nfam;
   const FamDev* fam;
   int nterm;
@@ -305,6 +324,11 @@ struct edk_operator {
   bool ff_ok = false;     // flip-flop bond-family fast path applies
   bool use_ff = true;     // callers may switch the fast path off (A/B checks)
   int tps = 1;            // threads per state of the fast path (1, 2 or 4; autotuned)
+  // row plan of the fast path on rank-searched sectors (edk_plan.cu): built on
+  // first use; plan_state 0 not built, 1 built, -1 not available
+  edk::DevBuf p_st, p_rk, p_rw, p_rkw, p_dg, p_binom, p_bad;
+  int plan_state = 0;
+  bool use_plan = true;   // tps == 1 on a rank-searched sector runs the plan kernel
   int use_block = -1;     // several right-hand sides through one SpMM: 1 yes, 0 no, -1 auto
                           // (matrix-free yes, materialised no: its SpMV already streams)
   std::vector<unsigned char> ff_params;
@@ -333,6 +357,12 @@ edk_status index_device(const BasisDev& dv, int64_t n, const uint64_t* s_d, int6
 bool rows_apply_ok(const edk_operator* op);
 edk_status apply_rows(edk_operator* op, int dtype, const void* x, void* y, int64_t row0,
                       int64_t row1, int accumulate, cudaStream_t st);
+// implemented in edk_plan.cu
+bool plan_applies(const edk_operator* op);
+edk_status plan_ensure(edk_operator* op);
+edk_status apply_plan(edk_operator* op, int dtype, const void* x, void* y, int64_t nvec,
+                      int64_t ldx, int64_t ldy, int accumulate, cudaStream_t st, int64_t row0,
+                      int64_t row1);
 // implemented in edk_sell.cu
 edk_status apply_sell_rows(edk_operator* op, int dtype, const void* x, void* y, int64_t row0,
                            int64_t row1, int accumulate, cudaStream_t st);
@@ -345,7 +375,8 @@ edk_status apply_device(edk_operator* op, int dtype, const void* x, void* y, int
 struct OpResult {
   std::vector<double> a, b, ev;  // recurrence coefficients and lowest Ritz values
   int steps = 0;
-  int status = 0;  // 0 ran to the step limit, 1 converged, 2 breakdown, 3 zero norm
+  int status = 0;  // 0 ran to the step limit, 1 converged, 2 breakdown, 3 zero norm,
+                   // 4 non-finite start
 };
 // ritz_out (optional, device): every operator's lowest Ritz vector in the
 // FP64 working dtype (F64 or C128), concatenated in operator order

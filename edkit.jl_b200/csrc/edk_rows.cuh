@@ -271,6 +271,244 @@ __device__ __forceinline__ uint32_t rank_after_swap(uint32_t s, uint32_t rs, int
   return ((s >> a) & 1u) ? rs + delta : rs - delta;  // modulo 2^32: the result is a valid rank
 }
 
+// Diagonal of bond family f on the bit planes X = s, Y = rotl(s, d), valid
+// mask V: sum over the local columns c = 2 X_p + Y_p of M[c][c] times the
+// number of bonds in column c, explicitly rounded.  Shared by every flip-flop
+// row kernel and the row-plan builder, so all of them round the diagonal alike.
+__device__ __forceinline__ void ff_diag(const FFParams& ff, int f, uint32_t X, uint32_t Y,
+                                        uint32_t V, double& dr, double& di) {
+  const double c0 = __popc(~X & ~Y & V), c1 = __popc(~X & Y & V), c2 = __popc(X & ~Y & V),
+               c3 = __popc(X & Y & V);
+  const double2* dv = ff.dval[f];
+  dr = __dadd_rn(dr, __fma_rn(dv[3].x, c3, __fma_rn(dv[2].x, c2, __fma_rn(dv[1].x, c1,
+                                                                          __dmul_rn(dv[0].x, c0)))));
+  di = __dadd_rn(di, __fma_rn(dv[3].y, c3, __fma_rn(dv[2].y, c2, __fma_rn(dv[1].y, c1,
+                                                                          __dmul_rn(dv[0].y, c0)))));
+}
+
+// diagonal-only generic terms (fields, zz on other sites) of row state st
+__device__ __forceinline__ void term_diag(const OpDev& op, uint32_t st, double& dr, double& di) {
+  for (int q = 0; q < op.nterm; ++q) {
+    const TermDev* T = op.term + q;
+    int c = 0;
+    for (int k = 0; k < T->nsites; ++k) c = (c << 1) | (int)((st >> T->bitpos[k]) & 1u);
+    const double2 dv = __ldg(op.dval + T->diag_off + c);
+    dr = __dadd_rn(dr, dv.x);
+    di = __dadd_rn(di, dv.y);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row body of the flip-flop fast path, shared by the tile kernels (rows sorted
+// per block at run time, any index search) and the row-plan kernels (rows
+// sorted once, rank-searched sectors).  For row i with state s:
+//   y_i = (1/R_i) sum_f conj(w_f) sum_hits conj(C_t) R_t x_t + diag_i x_i
+// where a hit exchanges the two sites of a bond of family f (value w_f =
+// M[2][1] = M[1][2]* of the local matrix), t is the target row, C_t the phase
+// index() returns and R_t its norm (TranslationalBasis.jl:310-341,
+// Operator.jl:426-465: H[t, i] = w C_t R_t / R_i; the product gathers the
+// conjugate, y_i = sum_t conj(H[t, i]) x_t, for a Hermitian operator).  Per
+// family the hits are summed first and multiplied by conj(w_f) once (per hit
+// when the two exchange values differ); 1/R_i is applied once at the end.
+// Every product is an explicitly rounded operation (no contraction left to the
+// compiler), so the tile and row-plan kernels, which share this body, give
+// bit-identical results.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double fma_(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double mul_(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_(float a, float b) { return __fmul_rn(a, b); }
+
+// Shared-memory tables of the fast kernels: binomials (rank updates) and the
+// coefficient table indexed by the low bits of a table value: coef[c] = R of
+// norm class c; with the rank table's shift M (k != 0) coef[M << 5 | c] =
+// C[M] R_c; with its sign bit (translation + parity) coef[sign << 5 | c] = +-R_c.
+template <int BK> struct FFTabSize { static constexpr int n = BK == BK_TRANS_RANK ? 1024 : 64; };
+template <int BK> struct FFTab {
+  uint32_t binom[32 * 33];
+  double2 coef[FFTabSize<BK>::n];
+};
+
+// binom_src: the 32 x 33 table in global memory, or null to compute it
+template <int BK>
+__device__ __forceinline__ void ff_tab_fill(FFTab<BK>& t, const BasisDev& b,
+                                            const uint32_t* binom_src) {
+  if (binom_src) {
+    for (int q = threadIdx.x; q < 32 * 33; q += blockDim.x) t.binom[q] = __ldg(binom_src + q);
+  } else {
+    fill_binom32(t.binom);
+  }
+  for (int q = threadIdx.x; q < FFTabSize<BK>::n; q += blockDim.x) {
+    const int c = q & 31;
+    const double R = (b.packed && c < b.nclass) ? b.Rcls[c] : 1.0;
+    double2 v = make_double2(R, 0.0);
+    if constexpr (BK == BK_TRANS_RANK) {
+      const int M = q >> 5;
+      const double2 C = M < b.len ? __ldg(b.phase + M) : make_double2(0.0, 0.0);
+      v = make_double2(C.x * R, C.y * R);
+    } else if constexpr (BK == BK_TRANSPAR_RANK) {
+      v = make_double2(((q >> 5) & 1) ? -R : R, 0.0);
+    }
+    t.coef[q] = v;
+  }
+}
+
+// S += conj(T) x for the target coefficient T = tr + i ti (real when !CT)
+template <class A, bool CX, bool CT>
+__device__ __forceinline__ void acc_t(Cx<A>& S, A tr, A ti, Cx<A> x) {
+  if constexpr (CT) {
+    S.r = fma_(ti, x.i, fma_(tr, x.r, S.r));
+    if constexpr (CX) S.i = fma_(-ti, x.r, fma_(tr, x.i, S.i));
+  } else {
+    S.r = fma_(tr, x.r, S.r);
+    if constexpr (CX) S.i = fma_(tr, x.i, S.i);
+  }
+}
+// Y += conj(w) S
+template <class A, bool CX>
+__device__ __forceinline__ void fold_w(Cx<A>& Y, double2 w, Cx<A> S) {
+  const A wr = (A)w.x, wi = (A)w.y;
+  if constexpr (CX) {
+    Y.r = fma_(wi, S.i, fma_(wr, S.r, Y.r));
+    Y.i = fma_(-wi, S.r, fma_(wr, S.i, Y.i));
+  } else {
+    Y.r = fma_(wr, S.r, Y.r);
+  }
+}
+
+// (ok, pos, coefficient) of the targets k1, k2 of a pair of hits: ranks
+// (rank table or complete sector) or states (tensor rows, canonicalise + probe).
+template <int BK, class A>
+__device__ __forceinline__ void ff_targets(const BasisDev& b, const FFTab<BK>& t, uint32_t k1,
+                                           uint32_t k2, bool two, bool& ok1, int64_t& pos1,
+                                           A& t1r, A& t1i, bool& ok2, int64_t& pos2, A& t2r,
+                                           A& t2i) {
+  constexpr bool RANKED = BK == BK_TRANS0_RANK || BK == BK_TRANS_RANK || BK == BK_TRANSPAR_RANK;
+  t1r = t2r = (A)1;
+  t1i = t2i = (A)0;
+  if constexpr (RANKED) {
+    constexpr uint32_t TM = FFTabSize<BK>::n - 1;
+    const uint32_t v1 = __ldg(b.rankmap + k1);
+    const uint32_t v2 = __ldg(b.rankmap + k2);
+    ok1 = v1 != ~0u;
+    ok2 = two && v2 != ~0u;
+    const int sh = b.rank_shift;
+    pos1 = ok1 ? (int64_t)(v1 >> sh) : 0;
+    pos2 = ok2 ? (int64_t)(v2 >> sh) : 0;
+    const double2 c1 = t.coef[v1 & TM], c2 = t.coef[v2 & TM];
+    t1r = (A)c1.x; t1i = (A)c1.y;
+    t2r = (A)c2.x; t2i = (A)c2.y;
+  } else if constexpr (BK == BK_PROJ_RANK || BK == BK_TENSOR) {  // k = the target's row
+    ok1 = true;
+    ok2 = two;
+    pos1 = (int64_t)k1;
+    pos2 = (int64_t)k2;
+  } else {  // k = the target state: canonicalise, then probe
+    HitCtx h1, h2;
+    canon_ctx<BK>(b, k1, h1);
+    canon_ctx<BK>(b, k2, h2);
+    double r1, r2;
+    locate2<BK>(b, t.binom, h1.key, h2.key, two, pos1, r1, ok1, pos2, r2, ok2);
+    if constexpr (BK != BK_PROJ_HASH) {
+      t1r = (A)(h1.pre * r1);
+      t1i = (A)(h1.pim * r1);
+      t2r = (A)(h2.pre * r2);
+      t2i = (A)(h2.pim * r2);
+    }
+  }
+}
+
+// Off-diagonal sum of one row (before the factor 1/R_i).  TPS lanes share the
+// row and take its pairs of hits in turn (lane `sub`); rkw, when not ~0u, is
+// the precomputed rank of the state with bits 0 and L-1 exchanged.
+template <int BK, class VT, int TPS>
+__device__ __forceinline__ Cx<typename VTraits<VT>::A> ff_row_sum(
+    const BasisDev& b, const FFParams& ff, const FFTab<BK>& t, uint32_t st, uint32_t rs,
+    uint32_t rkw, int sub, const VT* __restrict__ xk) {
+  using A = typename VTraits<VT>::A;
+  constexpr bool CX = VTraits<VT>::cx;
+  constexpr bool RANKED = BK == BK_TRANS0_RANK || BK == BK_TRANS_RANK || BK == BK_TRANSPAR_RANK;
+  constexpr bool BYRANK = RANKED || BK == BK_PROJ_RANK;
+  constexpr bool CT = BK == BK_TRANS_RANK || BK == BK_TRANS;  // complex target coefficients
+  const uint32_t mask = (uint32_t)b.maskL;
+  const int L = b.L;
+  Cx<A> Y{0, 0};
+  int pc = 0;  // pairs of hits seen so far in this row
+  for (int f = 0; f < ff.nfam; ++f) {
+    const int d = ff.d[f];
+    uint32_t bits = (st ^ rotl_L(st, d, L, mask)) & ff.valid[f];
+    const bool same = ff.same[f] != 0;
+    Cx<A> S0{0, 0};  // sum of conj(T) x (values equal), or of conj(w T) x (values differ)
+    // the target of hit p (sites p and p - d mod L): its rank, or its state
+    auto target = [&](int p) -> uint32_t {
+      const int q = p >= d ? p - d : p - d + L;
+      if constexpr (BYRANK) {
+        if (d == 1 && p != 0) {  // adjacent sites a = p - 1, a + 1: rank change C(a, j)
+          const int a = p - 1;
+          const uint32_t e = t.binom[a * 33 + __popc(st & ((1u << a) - 1u))];
+          return ((st >> a) & 1u) ? rs + e : rs - e;
+        }
+        if (d == 1 && rkw != ~0u) return rkw;
+        return rank_after_swap(st, rs, p, q, t.binom);
+      } else {
+        return st ^ (1u << p) ^ (1u << q);
+      }
+    };
+    while (bits) {
+      const int p1 = __ffs(bits) - 1;
+      bits &= bits - 1;
+      const bool two = bits != 0;
+      const int p2 = two ? __ffs(bits) - 1 : p1;
+      bits &= bits - 1;
+      if (TPS > 1 && (pc++ % TPS) != sub) continue;
+      const uint32_t k1 = target(p1), k2 = target(p2);
+      bool ok1, ok2;
+      int64_t pos1, pos2;
+      A t1r, t1i, t2r, t2i;
+      ff_targets<BK, A>(b, t, k1, k2, two, ok1, pos1, t1r, t1i, ok2, pos2, t2r, t2i);
+      const Cx<A> x1 = ldv(xk + pos1), x2 = ldv(xk + pos2);  // row 0 for an absent target
+      if (same) {
+        if (ok1) acc_t<A, CX, CT>(S0, t1r, t1i, x1);
+        if (ok2) acc_t<A, CX, CT>(S0, t2r, t2i, x2);
+      } else if constexpr (CX) {  // the two exchange values differ: fold w per hit
+        const double2 w1 = ((st >> p1) & 1u) ? ff.v2[f] : ff.v1[f];
+        const double2 w2 = ((st >> p2) & 1u) ? ff.v2[f] : ff.v1[f];
+        const A u1r = fma_(-(A)w1.y, t1i, mul_((A)w1.x, t1r)), u1i = fma_((A)w1.y, t1r, mul_((A)w1.x, t1i));
+        const A u2r = fma_(-(A)w2.y, t2i, mul_((A)w2.x, t2r)), u2i = fma_((A)w2.y, t2r, mul_((A)w2.x, t2i));
+        if (ok1) acc_t<A, CX, true>(S0, u1r, u1i, x1);
+        if (ok2) acc_t<A, CX, true>(S0, u2r, u2i, x2);
+      }
+    }
+    // (real vectors always see equal values: the two exchange elements of a
+    // Hermitian bond are complex conjugates, and complex operators refuse
+    // real vectors)
+    fold_w<A, CX>(Y, same ? ff.v1[f] : make_double2(1.0, 0.0), S0);
+  }
+  return Y;
+}
+
+// y_i (+)= invRi Y + diag x_i
+template <class VT>
+__device__ __forceinline__ void ff_row_store(Cx<typename VTraits<VT>::A> Y,
+                                             typename VTraits<VT>::A invRi, double dr, double di,
+                                             const VT* __restrict__ xk, VT* __restrict__ yk,
+                                             int64_t i, int accumulate) {
+  using A = typename VTraits<VT>::A;
+  constexpr bool CX = VTraits<VT>::cx;
+  const Cx<A> xi = ldv(xk + i);
+  Cx<A> out{fma_((A)dr, xi.r, mul_(invRi, Y.r)), (A)0};
+  if constexpr (CX) {
+    out.r = fma_((A)di, xi.i, out.r);
+    out.i = fma_(-(A)di, xi.r, fma_((A)dr, xi.i, mul_(invRi, Y.i)));
+  }
+  if (accumulate) {
+    const Cx<A> yo = ldout(yk + i);
+    out.r += yo.r;
+    out.i += yo.i;
+  }
+  stv(yk + i, out);
+}
+
 // 256 / TPS consecutive rows r0.. of the flip-flop fast path (one block of
 // 256 threads).  Rows are sorted by their number of off-diagonal hits so that
 // the lanes of a warp loop equally long; TPS adjacent lanes share one row and
@@ -282,21 +520,12 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
                                         VT* __restrict__ yk, int accumulate) {
   using A = typename VTraits<VT>::A;
   constexpr bool CX = VTraits<VT>::cx;
-  // BK_TRANS0_RANK / BK_TRANS_RANK: a translation sector whose target rows
-  // (and, with a momentum phase, shifts M) come from the rank table instead of
-  // canonicalisation + hash probe
-  constexpr bool PHASED = BK == BK_TRANS_RANK;
-  constexpr bool SIGNED = BK == BK_TRANSPAR_RANK;  // translation + parity: coefficient +-1
-  constexpr bool RANKED = BK == BK_TRANS0_RANK || PHASED || SIGNED;
-  constexpr int BKL = BK == BK_TRANS0_RANK ? (int)BK_TRANS0
-                      : (PHASED ? (int)BK_TRANS : (SIGNED ? (int)BK_TRANSPAR : BK));
-  __shared__ uint32_t s_binom[(BK == BK_PROJ_RANK || RANKED) ? 32 * 33 : 1];
+  constexpr bool RANKED = BK == BK_TRANS0_RANK || BK == BK_TRANS_RANK || BK == BK_TRANSPAR_RANK;
+  __shared__ FFTab<BK> s_tab;
   __shared__ int s_hist[64];
   __shared__ unsigned short s_order[256];
   __shared__ uint32_t s_state[256];
-  if constexpr (BK == BK_PROJ_RANK) fill_binom32(s_binom);
-  if constexpr (RANKED)
-    for (int q = threadIdx.x; q < 32 * 33; q += blockDim.x) s_binom[q] = __ldg(b.binom32 + q);
+  ff_tab_fill<BK>(s_tab, b, RANKED ? b.binom32 : nullptr);
   constexpr int RT = 256 / TPS;  // rows per tile
   const int t = threadIdx.x;
   if (t < 64) s_hist[t] = 0;
@@ -339,136 +568,23 @@ __device__ __forceinline__ void ff_tile(const BasisDev& b, const OpDev& op, cons
   if (TPS == 1 && !valid) return;
   const uint32_t st = s_state[tt];  // 0 past the last row: no hits
   const A invRi = (b.R && valid) ? (A)(1.0 / __ldg(b.R + i)) : (A)1;
-  // complete fixed-charge sector (BK_PROJ_RANK): a state's row is its colex
-  // rank, so target rows follow from the row index by the same rank update
-  constexpr bool DIRECT = BK == BK_PROJ_RANK;
-  uint32_t rs = 0;  // colex rank of the row state (rank-table search)
+  uint32_t rs = 0;  // colex rank of the row state (rank search), or the row (complete sector)
   if constexpr (RANKED) rs = valid ? __ldg(b.rowrank + i) : 0u;
-  if constexpr (DIRECT) rs = (uint32_t)i;
-  int pc = 0;  // pairs of hits seen so far in this row
-  double dr = 0.0, di = 0.0;
-  A ar = 0, ai = 0;
-  // bases whose index() coefficient has no phase (1 + 0i): the products with
-  // the phase are skipped (equal values; only the sign of a zero may differ)
-  // (translation + parity: a real +-1 phase, the imaginary products are skipped)
-  constexpr bool UNIT_PHASE =
-      BKL == BK_TENSOR || BKL == BK_PROJ_RANK || BKL == BK_PROJ_HASH || BKL == BK_TRANS0;
-  constexpr bool REAL_PHASE = BKL == BK_TRANSPAR;
-  auto acc = [&](const HitCtx& c, double rpos, double vr, double vi, Cx<A> xv) {
-    const A pr = (A)c.pre, pi = (A)c.pim, v_r = (A)vr, v_i = (A)vi;
-    const A ratio = (A)rpos * invRi;
-    const A cr = UNIT_PHASE ? v_r * ratio
-                 : REAL_PHASE ? (v_r * pr) * ratio : (v_r * pr - v_i * pi) * ratio;
-    if constexpr (CX) {
-      const A ci = UNIT_PHASE ? v_i * ratio
-                   : REAL_PHASE ? (v_i * pr) * ratio : (v_r * pi + v_i * pr) * ratio;
-      ar += cr * xv.r + ci * xv.i;
-      ai += cr * xv.i - ci * xv.r;
-    } else {
-      ar += cr * xv.r;
-    }
-  };
-  for (int f = 0; f < ff.nfam; ++f) {
-    const int d = ff.d[f];
-    const uint32_t X = st, Y = rotl_L(st, d, L, mask), V = ff.valid[f];
-    const uint32_t m1 = ~X & Y & V, m2 = X & ~Y & V;
-    const int c0 = __popc(~X & ~Y & V), c1 = __popc(m1), c2 = __popc(m2), c3 = __popc(X & Y & V);
-    dr += ff.dval[f][0].x * c0 + ff.dval[f][1].x * c1 + ff.dval[f][2].x * c2 + ff.dval[f][3].x * c3;
-    di += ff.dval[f][0].y * c0 + ff.dval[f][1].y * c1 + ff.dval[f][2].y * c2 + ff.dval[f][3].y * c3;
-    const double2 va = ff.v1[f], vb = ff.v2[f];
-    uint32_t bits = m1 | m2;
-    while (bits) {
-      const int p1 = __ffs(bits) - 1;
-      bits &= bits - 1;
-      const bool two = bits != 0;
-      const int p2 = two ? __ffs(bits) - 1 : p1;
-      if (two) bits &= bits - 1;
-      if (TPS > 1 && (pc++ % TPS) != sub) continue;
-      const int q1 = p1 >= d ? p1 - d : p1 - d + L, q2 = p2 >= d ? p2 - d : p2 - d + L;
-      HitCtx h1, h2;
-      int64_t pos1, pos2;
-      double rp1, rp2;
-      bool ok1, ok2;
-      if constexpr (RANKED || DIRECT) {
-        h1 = h2 = HitCtx{0u, 1.0, 0.0};
-        uint32_t k1, k2;
-        if (d == 1 && p1 != 0) {
-          // adjacent sites (p2 >= p1 > 0, no wrap-around): the bit at a = p - 1
-          // moves by one place, rank change C(a, j) with j set bits below a
-          const int a1 = p1 - 1, a2 = p2 - 1;
-          const uint32_t e1 = s_binom[a1 * 33 + __popc(st & ((1u << a1) - 1u))];
-          const uint32_t e2 = s_binom[a2 * 33 + __popc(st & ((1u << a2) - 1u))];
-          k1 = ((st >> a1) & 1u) ? rs + e1 : rs - e1;
-          k2 = ((st >> a2) & 1u) ? rs + e2 : rs - e2;
-        } else {
-          k1 = rank_after_swap(st, rs, p1, q1, s_binom);
-          k2 = two ? rank_after_swap(st, rs, p2, q2, s_binom) : k1;
-        }
-        if constexpr (DIRECT) {  // the exchange keeps the charge: both targets are rows
-          pos1 = (int64_t)k1;
-          pos2 = (int64_t)k2;
-          rp1 = rp2 = 1.0;
-          ok1 = true;
-          ok2 = two;
-        } else {
-          const uint32_t v1 = __ldg(b.rankmap + k1);
-          const uint32_t v2 = two ? __ldg(b.rankmap + k2) : ~0u;
-          ok1 = v1 != ~0u;
-          ok2 = v2 != ~0u;
-          pos1 = pos2 = 0;
-          rp1 = rp2 = 1.0;
-          int M1 = 0, M2 = 0;
-          if (ok1) rank_decode(b, v1, pos1, rp1, M1);
-          if (ok2) rank_decode(b, v2, pos2, rp2, M2);
-          if constexpr (PHASED) {  // phase C[M] of the target, as index() gives it
-            if (ok1) { const double2 c = __ldg(b.phase + M1); h1.pre = c.x; h1.pim = c.y; }
-            if (ok2) { const double2 c = __ldg(b.phase + M2); h2.pre = c.x; h2.pim = c.y; }
-          }
-          if constexpr (SIGNED) {  // bit 5 of the entry: the coefficient is -1
-            h1.pre = ((v1 >> 5) & 1u) ? -1.0 : 1.0;
-            h2.pre = ((v2 >> 5) & 1u) ? -1.0 : 1.0;
-          }
-        }
-      } else {
-        const uint32_t s1 = st ^ (1u << p1) ^ (1u << q1), s2 = st ^ (1u << p2) ^ (1u << q2);
-        canon_ctx<BKL>(b, s1, h1);
-        canon_ctx<BKL>(b, s2, h2);
-        locate2<BKL>(b, s_binom, h1.key, h2.key, two, pos1, rp1, ok1, pos2, rp2, ok2);
-      }
-      const Cx<A> x1 = ok1 ? ldv(xk + pos1) : Cx<A>{0, 0};
-      const Cx<A> x2 = ok2 ? ldv(xk + pos2) : Cx<A>{0, 0};
-      const double2 w1 = ((st >> p1) & 1u) ? vb : va;
-      const double2 w2 = ((st >> p2) & 1u) ? vb : va;
-      if (ok1) acc(h1, rp1, w1.x, w1.y, x1);
-      if (ok2) acc(h2, rp2, w2.x, w2.y, x2);
-    }
-  }
+  if constexpr (BK == BK_PROJ_RANK) rs = (uint32_t)i;
+  Cx<A> Y = ff_row_sum<BK, VT, TPS>(b, ff, s_tab, st, rs, ~0u, sub, xk);
   if constexpr (TPS > 1) {
 #pragma unroll
     for (int o = 1; o < TPS; o <<= 1) {
-      ar += __shfl_xor_sync(0xffffffffu, ar, o);
-      if constexpr (CX) ai += __shfl_xor_sync(0xffffffffu, ai, o);
+      Y.r += __shfl_xor_sync(0xffffffffu, Y.r, o);
+      if constexpr (CX) Y.i += __shfl_xor_sync(0xffffffffu, Y.i, o);
     }
     if (sub != 0 || !valid) return;
   }
-  for (int q = 0; q < op.nterm; ++q) {  // diagonal-only terms (fields, zz on other sites)
-    const TermDev* T = op.term + q;
-    int c = 0;
-    for (int k = 0; k < T->nsites; ++k) c = (c << 1) | (int)((st >> T->bitpos[k]) & 1u);
-    const double2 dv = __ldg(op.dval + T->diag_off + c);
-    dr += dv.x;
-    di += dv.y;
-  }
-  const Cx<A> xi = ldv(xk + i);
-  ar += (A)dr * xi.r + (A)di * xi.i;
-  if constexpr (CX) ai += (A)dr * xi.i - (A)di * xi.r;
-  Cx<A> out{ar, ai};
-  if (accumulate) {
-    const Cx<A> yo = ldout(yk + i);
-    out.r += yo.r;
-    out.i += yo.i;
-  }
-  stv(yk + i, out);
+  double dr = 0.0, di = 0.0;
+  for (int f = 0; f < ff.nfam; ++f)
+    ff_diag(ff, f, st, rotl_L(st, ff.d[f], L, mask), ff.valid[f], dr, di);
+  term_diag(op, st, dr, di);
+  ff_row_store<VT>(Y, invRi, dr, di, xk, yk, i, accumulate);
 }
 
 
