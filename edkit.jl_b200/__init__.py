@@ -5,9 +5,9 @@ The compute path is libedk.so (hand-written CUDA behind the C ABI in
 include/edk.h); this package is the Python mirror of the reference's Julia API.
 """
 from ._lib import EDKError, load as _load
-from .algorithms import (KrylovEvolutionDiagnostics, batch_lanczos_e0, block_lanczos, gapratio,
-                         ground_state, lanczos_e0, meangapratio, productstate, timeevolve,
-                         tridiag_eigen)
+from .algorithms import (KrylovEvolutionCache, KrylovEvolutionDiagnostics, batch_lanczos_e0,
+                         block_lanczos, gapratio, ground_state, lanczos_e0, meangapratio,
+                         productstate, timeevolve, tridiag_eigen)
 from .basis import (AbelianBasis, AbstractBasis, FlipBasis, ParityBasis, ParityFlipBasis,
                     ProjectedBasis, TensorBasis, TranslationalBasis, TranslationFlipBasis,
                     TranslationParityBasis, basis)
@@ -19,7 +19,7 @@ __all__ = [
     "AbelianBasis", "AbstractBasis", "ParityBasis", "FlipBasis", "ParityFlipBasis",
     "TranslationFlipBasis", "basis", "spin", "σ", "operator", "trans_inv_operator",
     "Operator", "mul", "mul_", "lanczos_e0", "ground_state", "batch_lanczos_e0", "block_lanczos",
-    "timeevolve",
+    "timeevolve", "KrylovEvolutionCache",
     "tridiag_eigen", "gapratio", "meangapratio", "productstate", "KrylovEvolutionDiagnostics", "version",
     "schmidt", "ent_spec", "entropy", "ent_S", "DoubleBasis", "symmetrizer",
 ]

@@ -30,7 +30,8 @@ EXPORTS = [
     "edk_block_lanczos_default_opts",
     "edk_apply", "edk_apply_async", "edk_lanczos_e0", "edk_krylov_default_opts",
     "edk_krylov_evolve", "edk_batch_lanczos_e0", "edk_tridiag_eigen", "edk_last_error",
-    "edk_version",
+    "edk_version", "edk_krylov_cache_create", "edk_krylov_cache_evolve", "edk_krylov_cache_info",
+    "edk_krylov_cache_destroy", "edk_selftest_bounded_wait",
 ]
 
 
@@ -158,6 +159,11 @@ def load():
         "edk_krylov_default_opts": (None, [C.POINTER(KrylovOpts)]),
         "edk_krylov_evolve": (st, [vp, C.POINTER(KrylovOpts), vp, vp, i64, vp, i32,
                                    C.POINTER(KrylovDiag)]),
+        "edk_krylov_cache_create": (st, [vp, C.POINTER(KrylovOpts), vp, i32, C.POINTER(vp)]),
+        "edk_krylov_cache_evolve": (st, [vp, vp, i64, vp, i32]),
+        "edk_krylov_cache_info": (st, [vp, dp, dp, C.POINTER(i32), C.POINTER(KrylovDiag)]),
+        "edk_krylov_cache_destroy": (st, [vp]),
+        "edk_selftest_bounded_wait": (st, [C.c_uint32]),
         "edk_batch_lanczos_e0": (st, [i32, vp, C.POINTER(LanczosOpts), vp, i32, vp,
                                       C.POINTER(LanczosDiag)]),
         "edk_tridiag_eigen": (C.c_int, [C.c_int, vp, vp, vp, vp]),

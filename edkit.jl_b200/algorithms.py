@@ -126,6 +126,101 @@ class KrylovEvolutionDiagnostics(dict):
         return self[k]
 
 
+def _krylov_opts(tol, m_init, m_max, extend_step, nsample, bisect_iters, reuse_basis,
+                 extend_basis, normalize_output, precision):
+    o = E.KrylovOpts()
+    E.load().edk_krylov_default_opts(C.byref(o))
+    o.tol, o.m_init, o.m_max, o.extend_step = tol, m_init, m_max, extend_step
+    o.nsample, o.bisect_iters = nsample, bisect_iters
+    o.reuse_basis, o.extend_basis = int(reuse_basis), int(extend_basis)
+    o.normalize_output = int(normalize_output)
+    o.precision = {"fp64": E.PREC_FP64, "mixed": E.PREC_MIXED}[precision]
+    return o
+
+
+def _krylov_diag(d):
+    return KrylovEvolutionDiagnostics(
+        basis_builds=d.basis_builds, basis_extensions=d.basis_extensions, restarts=d.restarts,
+        matvecs=d.matvecs, total_times_served=d.total_times_served, max_dim_used=d.max_dim_used,
+        accepted_intervals=list(d.accepted_intervals[: min(d.n_intervals, 64)]),
+        seconds=d.seconds)
+
+
+class KrylovEvolutionCache:
+    """KrylovEvolutionCache(H, ψ0; kwargs...) — TimeEvolution.jl:166-218.
+
+    A resumable propagator: the Lanczos basis, anchor state and diagnostics
+    live on the device between calls of ``timeevolve_``, which serves forward
+    times only (TimeEvolution.jl:586-636).  ψ0 is a host array or a CUDA
+    tensor; states come back the same way."""
+
+    def __init__(self, H: Operator, psi0, *, tol=1e-10, m_init=30, m_max=60, extend_step=10,
+                 nsample=13, bisect_iters=12, reuse_basis=True, extend_basis=True,
+                 normalize_output=False, precision="fp64"):
+        self.H = H
+        self.N = H.size(1)
+        self._dev = hasattr(psi0, "data_ptr") and getattr(psi0, "is_cuda", False)
+        if self._dev:
+            import torch
+            psi0 = psi0.to(torch.complex128).contiguous()
+            self._device = psi0.device
+        else:
+            psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
+        if psi0.shape[0] != self.N:
+            raise ValueError("psi0 has the wrong length")
+        o = _krylov_opts(tol, m_init, m_max, extend_step, nsample, bisect_iters, reuse_basis,
+                         extend_basis, normalize_output, precision)
+        h = C.c_void_p()
+        E.check(E.load().edk_krylov_cache_create(H._h, C.byref(o), E.ptr(psi0),
+                                                 E.DEVICE if self._dev else E.HOST, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            E.load().edk_krylov_cache_destroy(h)
+            self._h = None
+
+    def _info(self):
+        ta, tl, m = C.c_double(), C.c_double(), C.c_int32()
+        d = E.KrylovDiag()
+        E.check(E.load().edk_krylov_cache_info(self._h, C.byref(ta), C.byref(tl), C.byref(m),
+                                               C.byref(d)))
+        return ta.value, tl.value, m.value, d
+
+    @property
+    def t_anchor(self):
+        return self._info()[0]
+
+    @property
+    def t_latest(self):
+        return self._info()[1]
+
+    @property
+    def m(self):
+        return self._info()[2]
+
+    @property
+    def diagnostics(self):
+        return _krylov_diag(self._info()[3])
+
+    def timeevolve_(self, t):
+        """timeevolve!(cache, t) for a time, or timeevolve!(out, cache, ts) for a
+        non-decreasing sequence (columns in the order given)."""
+        scalar = np.isscalar(t)
+        ts = np.ascontiguousarray(np.atleast_1d(np.asarray(t, dtype=np.float64)))
+        if self._dev:
+            import torch
+            out = torch.empty((len(ts), self.N), dtype=torch.complex128, device=self._device)
+        else:
+            out = np.zeros((self.N, len(ts)), dtype=np.complex128, order="F")
+        E.check(E.load().edk_krylov_cache_evolve(self._h, E.ptr(ts), len(ts), E.ptr(out),
+                                                 E.DEVICE if self._dev else E.HOST))
+        if self._dev:
+            out = out.t()
+        return out[:, 0] if scalar else out
+
+
 def timeevolve(H: Operator, psi0, t, *, return_diagnostics=False, tol=1e-10, m_init=30,
                m_max=60, extend_step=10, nsample=13, bisect_iters=12, reuse_basis=True,
                extend_basis=True, normalize_output=False, precision="fp64"):
@@ -146,13 +241,8 @@ def timeevolve(H: Operator, psi0, t, *, return_diagnostics=False, tol=1e-10, m_i
         psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
     if psi0.shape[0] != D:
         raise ValueError("psi0 has the wrong length")
-    o = E.KrylovOpts()
-    E.load().edk_krylov_default_opts(C.byref(o))
-    o.tol, o.m_init, o.m_max, o.extend_step = tol, m_init, m_max, extend_step
-    o.nsample, o.bisect_iters = nsample, bisect_iters
-    o.reuse_basis, o.extend_basis = int(reuse_basis), int(extend_basis)
-    o.normalize_output = int(normalize_output)
-    o.precision = {"fp64": E.PREC_FP64, "mixed": E.PREC_MIXED}[precision]
+    o = _krylov_opts(tol, m_init, m_max, extend_step, nsample, bisect_iters, reuse_basis,
+                     extend_basis, normalize_output, precision)
     if on_device:  # states stay in HBM: column q of the (D, nts) view is time ts[q]
         out = torch.empty((len(ts), D), dtype=torch.complex128, device=psi0.device)
     else:
@@ -163,11 +253,7 @@ def timeevolve(H: Operator, psi0, t, *, return_diagnostics=False, tol=1e-10, m_i
                                        C.byref(d)))
     if on_device:
         out = out.t()
-    diag = KrylovEvolutionDiagnostics(
-        basis_builds=d.basis_builds, basis_extensions=d.basis_extensions, restarts=d.restarts,
-        matvecs=d.matvecs, total_times_served=d.total_times_served, max_dim_used=d.max_dim_used,
-        accepted_intervals=list(d.accepted_intervals[: min(d.n_intervals, 64)]),
-        seconds=d.seconds)
+    diag = _krylov_diag(d)
     res = out[:, 0] if scalar else out
     return (res, diag) if return_diagnostics else res
 

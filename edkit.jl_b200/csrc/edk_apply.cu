@@ -703,6 +703,10 @@ static edk_status staged_status(edk_operator* op) {
   int err = 0;
   EDK_TRY_CUDA(cudaMemcpy(&err, op->s_err.p, sizeof(int), cudaMemcpyDeviceToHost));
   if (err) {
+    // the device did not complete a bulk copy: never use the staged kernel on
+    // this operator again (later products take the plain materialised kernel)
+    op->sell_tma_ok = false;
+    op->sell_tma = false;
     set_error("apply: the staged materialised product timed out waiting for its copies");
     return EDK_TIMEOUT;
   }

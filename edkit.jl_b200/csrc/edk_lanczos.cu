@@ -637,6 +637,10 @@ static edk_status lanczos_common(edk_operator* op, const edk_lanczos_opts* opts,
   EDK_RETURN_IF(stage_vector(v0, v0_dtype, ptr_kind, D, E.wdt, start, st));
   double nrm = 0.0;
   EDK_RETURN_IF(E.set_start(start.p, E.wdt, &nrm));
+  if (!std::isfinite(nrm)) {
+    set_error("Initial state has non-finite entries (NaN or Inf)");
+    return EDK_INVALID_ARG;
+  }
   if (!(nrm > 0.0)) {
     set_error("Initial state has zero norm");
     return EDK_ZERO_NORM;
@@ -705,7 +709,7 @@ static edk_status lanczos_common(edk_operator* op, const edk_lanczos_opts* opts,
 // ---------------------------------------------------------------------------
 // Adaptive Krylov exp(-iHt) psi — TimeEvolution.jl:166-649
 // ---------------------------------------------------------------------------
-namespace {
+namespace edk {
 
 struct KrylovCacheDev {
   Engine E;
@@ -889,8 +893,6 @@ struct KrylovCacheDev {
   }
 };
 
-}  // namespace
-
 extern "C" void edk_krylov_default_opts(edk_krylov_opts* o) {
   if (!o) return;
   o->tol = 1e-10;
@@ -905,36 +907,27 @@ extern "C" void edk_krylov_default_opts(edk_krylov_opts* o) {
   o->precision = EDK_PREC_FP64;
 }
 
-extern "C" edk_status edk_krylov_evolve(edk_operator* op, const edk_krylov_opts* opts,
-                                        const void* psi0, const double* ts, int64_t nts,
-                                        void* out, int32_t ptr_kind, edk_krylov_diag* diag) {
-  EDK_CHECK_ARG(op && opts && psi0 && ts && out, "edk_krylov_evolve: NULL argument");
-  EDK_CHECK_ARG(nts >= 0, "edk_krylov_evolve: nts < 0");
+// checks of the KrylovEvolutionCache constructor (TimeEvolution.jl:178-189)
+static edk_status krylov_check(edk_operator* op, const edk_krylov_opts* opts) {
   if (!op->gather) {
     set_error("edk_krylov_evolve: the propagator is Hermitian-only; the operator is not "
               "Hermitian in this basis");
     return EDK_NOT_HERMITIAN;
   }
-  for (int64_t q = 0; q < nts; ++q)
-    if (ts[q] < 0) {
-      set_error("timeevolve: all times in ts must be non-negative; backward evolution is not "
-                "supported");
-      return EDK_BACKWARD_TIME;
-    }
-  const int64_t D = op->b->D;
-  EDK_CHECK_ARG(D > 0, "Initial state must be non-empty");
+  EDK_CHECK_ARG(op->b->D > 0, "Initial state must be non-empty");
   EDK_CHECK_ARG(opts->m_init >= 1, "m_init must be ≥ 1");
   EDK_CHECK_ARG(opts->m_max >= opts->m_init, "m_max must be ≥ m_init");
   EDK_CHECK_ARG(opts->nsample >= 2, "nsample must be ≥ 2");
   EDK_CHECK_ARG(opts->bisect_iters >= 0, "bisect_iters must be ≥ 0");
   EDK_CHECK_ARG(opts->extend_step >= 1, "extend_step must be ≥ 1");
-  std::lock_guard<std::mutex> lk(op->mu);
-  double t0 = now_s();
+  return EDK_OK;
+}
+
+// the constructor's set-up: anchor = psi0, V[:, 1] = psi0 / |psi0|, first basis
+static edk_status krylov_start(KrylovCacheDev& K, edk_operator* op, const edk_krylov_opts* opts,
+                               const void* psi0, int32_t ptr_kind, edk_krylov_diag* dg) {
+  const int64_t D = op->b->D;
   cudaStream_t st = op->stream;
-  edk_krylov_diag local{};
-  edk_krylov_diag* dg = diag ? diag : &local;
-  *dg = edk_krylov_diag{};
-  KrylovCacheDev K;
   K.o = *opts;
   K.dg = dg;
   K.m_max = (int)std::min<int64_t>(opts->m_max, D);
@@ -946,6 +939,10 @@ extern "C" edk_status edk_krylov_evolve(edk_operator* op, const edk_krylov_opts*
   EDK_RETURN_IF(stage_vector(psi0, EDK_C128, ptr_kind, D, EDK_C128, K.anchor, st));
   double nrm = 0.0;
   EDK_RETURN_IF(K.E.set_start(K.anchor.p, EDK_C128, &nrm));
+  if (!std::isfinite(nrm)) {
+    set_error("Initial state has non-finite entries (NaN or Inf)");
+    return EDK_INVALID_ARG;
+  }
   if (!(nrm > 0)) {
     set_error("Initial state has zero norm");
     return EDK_ZERO_NORM;
@@ -955,16 +952,19 @@ extern "C" edk_status edk_krylov_evolve(edk_operator* op, const edk_krylov_opts*
   EDK_RETURN_IF(K.reduced());
   dg->basis_builds += 1;
   dg->max_dim_used = std::max(dg->max_dim_used, K.m);
-  // serve times in sorted order, write columns in the caller's order
-  std::vector<int64_t> perm(nts);
-  std::iota(perm.begin(), perm.end(), 0);
-  std::stable_sort(perm.begin(), perm.end(), [&](int64_t a, int64_t b) { return ts[a] < ts[b]; });
-  DevBuf psi;
-  EDK_RETURN_IF(psi.alloc((size_t)D * 16));
+  return EDK_OK;
+}
+
+// timeevolve!(cache, t) for each t of a non-decreasing sequence (:586-636):
+// column p of out (device) or of the host array receives the state at ts[p]
+static edk_status krylov_serve(KrylovCacheDev& K, edk_operator* op, const double* ts, int64_t nts,
+                               const int64_t* perm, void* out, int32_t ptr_kind, DevBuf& psi) {
+  const int64_t D = op->b->D;
+  cudaStream_t st = op->stream;
   for (int64_t q = 0; q < nts; ++q) {
-    int64_t p = perm[q];
-    double tf = ts[p];
-    double tau = tf - K.t_anchor;
+    const int64_t p = perm ? perm[q] : q;
+    const double tf = ts[p];
+    const double tau = tf - K.t_anchor;
     EDK_RETURN_IF(K.ensure(tau));
     void* dst = (ptr_kind == EDK_DEVICE) ? (void*)((double2*)out + (size_t)p * D) : psi.p;
     EDK_RETURN_IF(K.reconstruct(tf - K.t_anchor, dst));
@@ -972,9 +972,120 @@ extern "C" edk_status edk_krylov_evolve(edk_operator* op, const edk_krylov_opts*
       EDK_TRY_CUDA(cudaMemcpyAsync((double2*)out + (size_t)p * D, psi.p, (size_t)D * 16,
                                    cudaMemcpyDeviceToHost, st));
     K.t_latest = tf;
-    dg->total_times_served += 1;
+    K.dg->total_times_served += 1;
   }
   EDK_TRY_CUDA(cudaStreamSynchronize(st));
+  return EDK_OK;
+}
+
+}  // namespace edk
+
+struct edk_krylov_cache {
+  edk_operator* op = nullptr;
+  edk::KrylovCacheDev K;
+  edk_krylov_diag diag{};
+  edk::DevBuf psi;  // staging column of the host path
+  double seconds = 0.0;
+};
+
+extern "C" edk_status edk_krylov_evolve(edk_operator* op, const edk_krylov_opts* opts,
+                                        const void* psi0, const double* ts, int64_t nts,
+                                        void* out, int32_t ptr_kind, edk_krylov_diag* diag) {
+  EDK_CHECK_ARG(op && opts && psi0 && ts && out, "edk_krylov_evolve: NULL argument");
+  EDK_CHECK_ARG(nts >= 0, "edk_krylov_evolve: nts < 0");
+  EDK_CHECK_ARG(ptr_kind == EDK_HOST || ptr_kind == EDK_DEVICE, "edk_krylov_evolve: bad ptr_kind");
+  for (int64_t q = 0; q < nts; ++q)
+    if (ts[q] < 0) {
+      set_error("timeevolve: all times in ts must be non-negative; backward evolution is not "
+                "supported");
+      return EDK_BACKWARD_TIME;
+    }
+  EDK_RETURN_IF(krylov_check(op, opts));
+  std::lock_guard<std::mutex> lk(op->mu);
+  double t0 = now_s();
+  const int64_t D = op->b->D;
+  edk_krylov_diag local{};
+  edk_krylov_diag* dg = diag ? diag : &local;
+  *dg = edk_krylov_diag{};
+  KrylovCacheDev K;
+  EDK_RETURN_IF(krylov_start(K, op, opts, psi0, ptr_kind, dg));
+  // serve times in sorted order, write columns in the caller's order
+  std::vector<int64_t> perm(nts);
+  std::iota(perm.begin(), perm.end(), 0);
+  std::stable_sort(perm.begin(), perm.end(), [&](int64_t a, int64_t b) { return ts[a] < ts[b]; });
+  DevBuf psi;
+  if (ptr_kind == EDK_HOST) EDK_RETURN_IF(psi.alloc((size_t)D * 16));
+  EDK_RETURN_IF(krylov_serve(K, op, ts, nts, perm.data(), out, ptr_kind, psi));
   dg->seconds = now_s() - t0;
+  return EDK_OK;
+}
+
+extern "C" edk_status edk_krylov_cache_create(edk_operator* op, const edk_krylov_opts* opts,
+                                              const void* psi0, int32_t ptr_kind,
+                                              edk_krylov_cache** out) {
+  EDK_CHECK_ARG(out != nullptr, "edk_krylov_cache_create: out is NULL");
+  *out = nullptr;
+  EDK_CHECK_ARG(op && opts && psi0, "edk_krylov_cache_create: NULL argument");
+  EDK_CHECK_ARG(ptr_kind == EDK_HOST || ptr_kind == EDK_DEVICE,
+                "edk_krylov_cache_create: bad ptr_kind");
+  EDK_RETURN_IF(krylov_check(op, opts));
+  std::lock_guard<std::mutex> lk(op->mu);
+  double t0 = now_s();
+  auto* c = new edk_krylov_cache;
+  std::unique_ptr<edk_krylov_cache> guard(c);
+  c->op = op;
+  EDK_RETURN_IF(krylov_start(c->K, op, opts, psi0, ptr_kind, &c->diag));
+  c->seconds = now_s() - t0;
+  c->diag.seconds = c->seconds;
+  *out = guard.release();
+  return EDK_OK;
+}
+
+extern "C" edk_status edk_krylov_cache_evolve(edk_krylov_cache* c, const double* ts, int64_t nts,
+                                              void* out, int32_t ptr_kind) {
+  EDK_CHECK_ARG(c && ts && out, "edk_krylov_cache_evolve: NULL argument");
+  EDK_CHECK_ARG(nts >= 0, "edk_krylov_cache_evolve: nts < 0");
+  EDK_CHECK_ARG(ptr_kind == EDK_HOST || ptr_kind == EDK_DEVICE,
+                "edk_krylov_cache_evolve: bad ptr_kind");
+  for (int64_t q = 1; q < nts; ++q)
+    if (ts[q] < ts[q - 1]) {
+      set_error("timeevolve!: ts must be sorted in ascending order");
+      return EDK_INVALID_ARG;
+    }
+  for (int64_t q = 0; q < nts; ++q) {
+    if (!(ts[q] >= c->K.t_latest)) {
+      char msg[256];
+      std::snprintf(msg, sizeof msg,
+                    "timeevolve!: requested time %.17g precedes the last served time %.17g; "
+                    "backward evolution is not supported", ts[q], c->K.t_latest);
+      set_error(msg);
+      return EDK_BACKWARD_TIME;
+    }
+  }
+  edk_operator* op = c->op;
+  std::lock_guard<std::mutex> lk(op->mu);
+  double t0 = now_s();
+  if (ptr_kind == EDK_HOST && !c->psi.p) EDK_RETURN_IF(c->psi.alloc((size_t)op->b->D * 16));
+  c->K.dg = &c->diag;
+  edk_status rc = krylov_serve(c->K, op, ts, nts, nullptr, out, ptr_kind, c->psi);
+  c->seconds += now_s() - t0;
+  c->diag.seconds = c->seconds;
+  return rc;
+}
+
+extern "C" edk_status edk_krylov_cache_info(const edk_krylov_cache* c, double* t_anchor,
+                                            double* t_latest, int32_t* m, edk_krylov_diag* diag) {
+  EDK_CHECK_ARG(c != nullptr, "edk_krylov_cache_info: NULL cache");
+  if (t_anchor) *t_anchor = c->K.t_anchor;
+  if (t_latest) *t_latest = c->K.t_latest;
+  if (m) *m = c->K.m;
+  if (diag) *diag = c->diag;
+  return EDK_OK;
+}
+
+extern "C" edk_status edk_krylov_cache_destroy(edk_krylov_cache* c) {
+  if (!c) return EDK_OK;
+  std::lock_guard<std::mutex> lk(c->op->mu);  // device buffers go back while the operator is locked
+  delete c;
   return EDK_OK;
 }

@@ -193,6 +193,23 @@ __global__ void __launch_bounds__(256) k_sell_apply(BasisDev b, SellDev sd,
                          y + (int64_t)blockIdx.y * ldy, accumulate);
 }
 
+// Failure-detection self-test of the bounded waits the staged kernel uses: one
+// block waits on a shared-memory mbarrier whose phase nothing completes (it
+// expects two arrivals and receives one), with the same bounded poll; the
+// wait runs out, the block records the time-out in *err and returns.  No copy
+// is issued, so nothing is in flight when the block exits.
+__global__ void k_wait_selftest(uint32_t polls, int* __restrict__ err) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 2);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_arrive(&bar);
+  const bool ok = mbar_wait_bounded(&bar, 0u, polls);
+  if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicExch(err, 1);
+}
+
 // Materialised product with the entry stream staged through shared memory:
 // a persistent block walks windows wbeg + blockIdx.x + i * gridDim.x; thread 0
 // copies each window's packed entries (8 slices, contiguous in `col`) with one
@@ -246,7 +263,15 @@ __global__ void __launch_bounds__(256) k_sell_tma(BasisDev b, SellDev sd,
     const int stage = i & 1;
     const bool ok = mbar_wait_bounded(&bar[stage], (uint32_t)((i >> 1) & 1), 1u << 20);
     if (__syncthreads_or(!ok)) {
+      // a copy that does not complete means the device is already in a bad
+      // state; record it, give this block's copies in flight (this window's
+      // and, when one was issued, the next window's) another bounded wait, and
+      // stop
       if (t == 0) atomicExch(err, 1);
+      mbar_wait_bounded(&bar[stage], (uint32_t)((i >> 1) & 1), 1u << 20);
+      if (w + step < wend)
+        mbar_wait_bounded(&bar[stage ^ 1], (uint32_t)(((i + 1) >> 1) & 1), 1u << 20);
+      __syncthreads();
       return;
     }
     const int64_t slice = w * 8 + warp;
@@ -860,5 +885,33 @@ extern "C" edk_status edk_operator_materialize(edk_operator* op, int32_t enable,
   }
   if (!op->sell_ok) EDK_RETURN_IF(materialize(op));
   if (entries) *entries = op->sell_entries;
+  return EDK_OK;
+}
+
+extern "C" edk_status edk_selftest_bounded_wait(uint32_t polls) {
+  EDK_CHECK_ARG(polls >= 1 && polls <= (1u << 24),
+                "edk_selftest_bounded_wait: polls out of 1..2^24");
+  DevBuf err;
+  EDK_RETURN_IF(err.alloc(sizeof(int)));
+  cudaStream_t st = nullptr;
+  EDK_TRY_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  int flag = 0;
+  cudaError_t e = cudaMemsetAsync(err.p, 0, sizeof(int), st);
+  if (e == cudaSuccess) {
+    edk::k_wait_selftest<<<1, 128, 0, st>>>(polls, err.as<int>());
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, err.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  if (e != cudaSuccess) {
+    set_error(std::string("edk_selftest_bounded_wait: ") + cudaGetErrorString(e));
+    return EDK_CUDA_ERROR;
+  }
+  if (flag) {
+    set_error("bounded wait ran out after " + std::to_string(polls) +
+              " polls: the awaited barrier phase never completed (self-test)");
+    return EDK_TIMEOUT;
+  }
   return EDK_OK;
 }

@@ -366,6 +366,28 @@ edk_status edk_krylov_evolve(edk_operator* op, const edk_krylov_opts* opts, cons
                              const double* ts, int64_t nts, void* out, int32_t ptr_kind,
                              edk_krylov_diag* diag);
 
+/* Resumable Krylov evolution: the handle form of KrylovEvolutionCache
+ * (TimeEvolution.jl:166-218) with timeevolve!(cache, t) and
+ * timeevolve!(out, cache, ts) (TimeEvolution.jl:586-636).  create() checks the
+ * options as the constructor does, stages psi0 (EDK_C128, host or device per
+ * ptr_kind) as the anchor and builds the first Lanczos basis on the device.
+ * evolve() advances the cache forward: ts must be non-decreasing and not
+ * before the last time served (EDK_BACKWARD_TIME otherwise, with the
+ * reference's message); out receives N x nts complex columns (EDK_C128,
+ * host or device per ptr_kind).  The basis, the anchor and the diagnostics
+ * carry over from call to call.  info() reports the anchor time, the last
+ * served time, the current basis dimension and the accumulated diagnostics.
+ * The operator must outlive the handle; calls on one handle are serialised
+ * with the operator's other calls. */
+typedef struct edk_krylov_cache edk_krylov_cache;
+edk_status edk_krylov_cache_create(edk_operator* op, const edk_krylov_opts* opts,
+                                   const void* psi0, int32_t ptr_kind, edk_krylov_cache** out);
+edk_status edk_krylov_cache_evolve(edk_krylov_cache* cache, const double* ts, int64_t nts,
+                                   void* out, int32_t ptr_kind);
+edk_status edk_krylov_cache_info(const edk_krylov_cache* cache, double* t_anchor,
+                                 double* t_latest, int32_t* m, edk_krylov_diag* diag);
+edk_status edk_krylov_cache_destroy(edk_krylov_cache* cache);
+
 /* Batched Lanczos over independent operators (momentum sectors of one chain,
  * or disorder instances): all matvecs of one step run as ONE kernel launch
  * over a tile queue, the whole step is captured in a CUDA graph.  v0s holds
@@ -374,6 +396,14 @@ edk_status edk_krylov_evolve(edk_operator* op, const edk_krylov_opts* opts, cons
 edk_status edk_batch_lanczos_e0(int32_t nops, edk_operator* const* ops,
                                 const edk_lanczos_opts* opts, const void* v0s, int32_t v0_dtype,
                                 double* evals, edk_lanczos_diag* diag);
+
+/* Failure-detection self-test of the library's bounded device waits (the
+ * staged materialised product's copy waits use the same helper): one block
+ * waits, with a limit of `polls` polls, on a shared-memory barrier that
+ * nothing completes, records the time-out and returns.  Returns EDK_TIMEOUT
+ * with a message, and leaves the context usable, when the limit works.  No
+ * reference counterpart (EDKit has no device waits). */
+edk_status edk_selftest_bounded_wait(uint32_t polls);
 
 /* Symmetric tridiagonal eigensolver used by the Lanczos/Krylov drivers
  * (eigen(SymTridiagonal(a, b)), TimeEvolution.jl:311-323): diagonal a[m],
