@@ -22,7 +22,7 @@ import Base: *, size, eltype
 import LinearAlgebra: mul!
 
 export B200Operator, B200Basis, lanczos_e0, ground_state, timeevolve, autotune!, block_lanczos,
-       set_search!,
+       set_search!, KrylovCacheB200, timeevolve!,
        schmidt_b200, ent_S_b200, double_basis_b200, symmetrizer_b200
 
 const libedk = get(ENV, "EDK_LIB", joinpath(@__DIR__, "..", "libedk.so"))
@@ -73,36 +73,79 @@ dtype_code(::Type{ComplexF32}) = Int32(3)
 
 # Basis kind and parameters from the Julia basis object; the tables b.I, b.R
 # are passed as EDKit holds them, so the device copy is the same table.
+# Symmetry-group bases (AbelianBasis, i.e. every `basis(...)` with k/p/z or
+# `symmetries`, and the dedicated Parity/Flip/ParityFlip/TranslationFlip
+# types) also pass their generators: order, quantum number, site
+# permutation (site i -> perm[i]) and spin-inversion flags, in the order
+# AbelianOperator holds them (AbelianBasis.jl:143-193, 771-833).
+struct Gens
+    order::Vector{Int32}; q::Vector{Int32}; perm::Vector{Int32}; inv::Vector{UInt8}
+end
+Gens() = Gens(Int32[], Int32[], Int32[], UInt8[])
+function push_gen!(G::Gens, order, q, perm, inv)
+    push!(G.order, order); push!(G.q, q)
+    append!(G.perm, Int32.(perm)); append!(G.inv, UInt8.(inv))
+    G
+end
+# quantum number of a cyclic generator from its phase table c[j] = exp(2πi q j/order)
+gen_q(c, order) = order == 1 ? 0 : mod(round(Int, angle(ComplexF64(c[2])) * order / (2π)), order)
+# internal momentum K of a translation phase table C[j] = exp(-2πi K j/len)
+mom_K(C, len) = length(C) > 1 ? mod(round(Int, -angle(ComplexF64(C[2])) * len / (2π)), len) : 0
+reflection(L) = collect(L:-1:1)
+
 function basis_desc(b)
     L = length(b.dgt)
+    G = Gens()
     kind, a, k, p = if b isa TensorBasis
         0, 1, 0, 1
     elseif b isa ProjectedBasis
         1, 1, 0, 1
     elseif b isa TranslationalBasis
-        # b.C encodes k = mod(-k, len); pass k through C[2] is ambiguous, so
-        # the caller's k is recovered from the phase of C[2]
         len = L ÷ b.A
-        kk = length(b.C) > 1 ? round(Int, -angle(ComplexF64(b.C[2])) * len / (2π)) : 0
-        2, b.A, mod(-kk, len), 1
+        2, b.A, mod(-mom_K(b.C, len), len), 1   # the caller's k (the library takes mod(-k, len))
     elseif b isa TranslationParityBasis
         len = L ÷ b.A
         3, b.A, (all(isone, b.C) ? 0 : len ÷ 2), b.P
+    elseif b isa AbelianBasis
+        Gop = b.G
+        for g in eachindex(Gop.g)
+            push_gen!(G, Gop.g[g], gen_q(Gop.c[g], Gop.g[g]), Gop.perm[g], Gop.inv[g])
+        end
+        4, 1, 0, 1
+    elseif b isa ParityBasis
+        push_gen!(G, 2, b.P == -1 ? 1 : 0, reflection(L), zeros(Bool, L))
+        4, 1, 0, 1
+    elseif b isa FlipBasis
+        push_gen!(G, 2, b.P == -1 ? 1 : 0, collect(1:L), ones(Bool, L))
+        4, 1, 0, 1
+    elseif b isa ParityFlipBasis
+        push_gen!(G, 2, b.P == -1 ? 1 : 0, reflection(L), zeros(Bool, L))
+        push_gen!(G, 2, b.Z == -1 ? 1 : 0, collect(1:L), ones(Bool, L))
+        4, 1, 0, 1
+    elseif b isa TranslationFlipBasis
+        len = L ÷ b.A
+        perm = [mod(i - b.A - 1, L) + 1 for i in 1:L]   # translation by the unit cell
+        push_gen!(G, len, mom_K(b.C, len), perm, zeros(Bool, L))
+        push_gen!(G, 2, b.P == -1 ? 1 : 0, collect(1:L), ones(Bool, L))
+        5, 1, 0, 1
     else
         error("B200Operator: basis type $(typeof(b)) is not on the GPU path")
     end
-    return kind, L, Int32(b.B), a, k, p
+    return kind, L, Int32(b.B), a, k, p, G
 end
 
 mutable struct B200Basis
     h::Ptr{Cvoid}
     function B200Basis(b)
-        kind, L, base, a, k, p = basis_desc(b)
+        kind, L, base, a, k, p, G = basis_desc(b)
         I = kind == 0 ? Int64[] : Vector{Int64}(b.I)
         R = kind <= 1 ? Float64[] : Vector{Float64}(b.R)
-        GC.@preserve I R begin
-            d = BasisDesc(kind, L, base, a, k, p, -1, 0, C_NULL, C_NULL, C_NULL, C_NULL, C_NULL,
-                          length(I), kind == 0 ? C_NULL : pointer(I),
+        ngen = length(G.order)
+        GC.@preserve I R G begin
+            d = BasisDesc(kind, L, base, a, k, p, -1, ngen,
+                          ngen == 0 ? C_NULL : pointer(G.order), ngen == 0 ? C_NULL : pointer(G.q),
+                          ngen == 0 ? C_NULL : pointer(G.perm), ngen == 0 ? C_NULL : pointer(G.inv),
+                          C_NULL, length(I), kind == 0 ? C_NULL : pointer(I),
                           kind <= 1 ? C_NULL : pointer(R))
             out = Ref{Ptr{Cvoid}}(C_NULL)
             check(ccall((:edk_basis_create, libedk), Cint, (Ref{BasisDesc}, Ref{Ptr{Cvoid}}), d, out))
@@ -226,6 +269,42 @@ function timeevolve(H::B200Operator, ψ0::AbstractVector, ts::AbstractVector{<:R
          Int32, Ref{KrylovDiag}), H.h, o, ψ, t, length(t), out, 0, d))
     return_diagnostics ? (out, d) : out
 end
+"""
+    KrylovCacheB200(H::B200Operator, ψ0; tol=1e-10, m_init=30, m_max=60, ...)
+
+KrylovEvolutionCache on the GPU (TimeEvolution.jl:166-218); advance it with
+`timeevolve!(cache, t)` or `timeevolve!(cache, ts)` (forward times only).
+"""
+mutable struct KrylovCacheB200
+    h::Ptr{Cvoid}
+    H::B200Operator
+    N::Int
+    function KrylovCacheB200(H::B200Operator, ψ0::AbstractVector; tol=1e-10, m_init=30,
+                             m_max=60, extend_step=10, nsample=13, bisect_iters=12,
+                             reuse_basis=true, extend_basis=true, normalize_output=false,
+                             precision::Symbol=:fp64)
+        ψ = Vector{ComplexF64}(ψ0)
+        o = KrylovOpts(tol, m_init, m_max, extend_step, nsample, bisect_iters, reuse_basis,
+                       extend_basis, normalize_output, precision === :mixed ? 1 : 0)
+        out = Ref{Ptr{Cvoid}}(C_NULL)
+        GC.@preserve ψ check(ccall((:edk_krylov_cache_create, libedk), Cint,
+            (Ptr{Cvoid}, Ref{KrylovOpts}, Ptr{ComplexF64}, Int32, Ref{Ptr{Cvoid}}),
+            H.h, o, ψ, 0, out))
+        obj = new(out[], H, length(ψ))
+        finalizer(x -> ccall((:edk_krylov_cache_destroy, libedk), Cint, (Ptr{Cvoid},), x.h), obj)
+        obj
+    end
+end
+
+function timeevolve!(c::KrylovCacheB200, ts::AbstractVector{<:Real})
+    t = Vector{Float64}(ts)
+    out = Matrix{ComplexF64}(undef, c.N, length(t))
+    GC.@preserve t out check(ccall((:edk_krylov_cache_evolve, libedk), Cint,
+        (Ptr{Cvoid}, Ptr{Float64}, Int64, Ptr{ComplexF64}, Int32), c.h, t, length(t), out, 0))
+    out
+end
+timeevolve!(c::KrylovCacheB200, t::Real) = timeevolve!(c, [t])[:, 1]
+
 # sparse!(opt) / clear_sparse_cache! (Operator.jl:221-285) on the device
 function EDKit.sparse!(H::B200Operator)
     n = Ref{Int64}(0)
