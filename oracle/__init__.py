@@ -77,6 +77,12 @@ def lib():
         L.orc_gosper_next.argtypes = [C.c_uint64]
         L.orc_apply_perm_benes.restype = C.c_uint64
         L.orc_apply_perm_benes.argtypes = [vp, i32, C.c_uint64]
+        L.orc_translational_tables.restype = vp
+        L.orc_translational_tables.argtypes = [i32, i32, i32, i32, i64, vp, vp]
+        L.orc_trans_judge.argtypes = [i32, i32, i32, i32, i32, i64, vp, vp, vp]
+        L.orc_rows_hermitian.argtypes = [vp, i64, vp, vp, vp]
+        L.orc_coo.restype = i64
+        L.orc_coo.argtypes = [vp, vp, vp, vp]
         L.orc_num_threads.restype = i32
         L.orc_set_threads.argtypes = [i32]
         _lib = L
@@ -244,6 +250,26 @@ def translational(L, k=0, N=None, a=1, f=None, base=2, threaded=True, gosper=Tru
     ob = OBasis(h, L, base, keep)
     ob.A = a
     return ob
+
+
+def translational_from_tables(L, I, R, k=0, a=1, base=2):
+    """TranslationalBasis over given tables (1-based I, R) — for sectors too
+    large to scan here; check the tables with trans_judge."""
+    I = np.ascontiguousarray(I, dtype=np.int64)
+    R = np.ascontiguousarray(R, dtype=np.float64)
+    h = lib().orc_translational_tables(L, base, k, a, len(I), _ptr(I), _ptr(R))
+    return OBasis(h, L, base, (I, R))
+
+
+def trans_judge(L, idx, k=0, N=None, a=1, base=2):
+    """The TranslationalBasis judge (TranslationalBasis.jl:94-114) on 1-based
+    indices: (accepted, norm) per index."""
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    acc = np.zeros(len(idx), np.uint8)
+    R = np.zeros(len(idx), np.float64)
+    lib().orc_trans_judge(L, base, k, -1 if N is None else N, a, len(idx), _ptr(idx), _ptr(acc),
+                          _ptr(R))
+    return acc.astype(bool), R
 
 
 def transparity(L, k=0, p=1, N=None, a=1, f=None, base=2, threaded=True, gosper=True):
@@ -596,6 +622,29 @@ class OOperator:
         lib().orc_mul_cols(self.h, _ptr(X), _ptr(Y), X.shape[1], int(j0), int(j1), int(nthreads))
         return Y
 
+    def sparse(self):
+        """H as a scipy CSR matrix of the entries colmn! scatters (duplicates
+        summed, the way the scatter accumulates them)."""
+        import scipy.sparse as sp
+        n = lib().orc_coo(self.h, None, None, None)
+        r = np.zeros(n, np.int64)
+        c = np.zeros(n, np.int64)
+        v = np.zeros(2 * n, np.float64)
+        lib().orc_coo(self.h, _ptr(r), _ptr(c), _ptr(v))
+        M = sp.coo_matrix((v[0::2] + 1j * v[1::2], (r - 1, c - 1)),
+                          shape=(self.dim, self.dim)).tocsr()
+        M.sum_duplicates()
+        return M
+
+    def rows_hermitian(self, rows, x):
+        """(H*x)[rows] (1-based rows) of a Hermitian operator, each from the
+        conjugated column colmn! builds (orc_rows_hermitian)."""
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        X = np.ascontiguousarray(np.asarray(x, dtype=np.complex128))
+        Y = np.zeros(len(rows), np.complex128)
+        lib().orc_rows_hermitian(self.h, len(rows), _ptr(rows), _ptr(X), _ptr(Y))
+        return Y
+
     def mul_serial(self, x, y=None):
         """mul!(y, opt, x): single-threaded, accumulates into y."""
         x = np.asarray(x)
@@ -700,9 +749,43 @@ def tridiag_eigen(alpha, beta):
     return eigh_tridiagonal(alpha, beta[: m - 1])
 
 
-def lanczos_e0(apply, v1, m, nev=1):
-    """E0 (and the lowest nev Ritz values) after m CGS2 Lanczos steps."""
-    a, b, _, mu, _ = lanczos_build(apply, v1, m)
+def lanczos_build_blas(apply, v1, m, dtype=np.float64):
+    """The same m steps with each of the two full sweeps taken as one block
+    projection (w -= V (V^H w), through BLAS) instead of one column at a time:
+    the same subspace in exact arithmetic, fast enough for sectors of a
+    million rows.  Returns (alpha, beta, m_used)."""
+    N = v1.shape[0]
+    V = np.zeros((m + 1, N), dtype=dtype)  # row j = v_j
+    V[0] = v1 / np.linalg.norm(v1)
+    alpha = np.zeros(m); beta = np.zeros(m)
+    for j in range(m):
+        w = np.array(apply(V[j]), dtype=dtype)
+        if j > 0:
+            w -= beta[j - 1] * V[j - 1]
+        aj = float(np.real(np.vdot(V[j], w)))
+        alpha[j] = aj
+        w -= aj * V[j]
+        Vj = V[: j + 1]
+        for _ in range(2):
+            w -= (Vj.conj() @ w) @ Vj
+        bj = float(np.linalg.norm(w))
+        beta[j] = bj
+        if bj <= math.sqrt(np.finfo(np.float64).eps) * max(1.0, abs(aj)):
+            beta[j] = 0.0
+            return alpha[: j + 1], beta[: j + 1], j + 1
+        V[j + 1] = w * (1.0 / bj)
+    return alpha, beta, m
+
+
+def lanczos_e0(apply, v1, m, nev=1, blas=False):
+    """E0 (and the lowest nev Ritz values) after m CGS2 Lanczos steps
+    (blas=True: the block-projection form of the same sweeps, real vectors
+    when v1 is real)."""
+    if blas:
+        dt = np.complex128 if np.iscomplexobj(v1) else np.float64
+        a, b, _ = lanczos_build_blas(apply, v1, m, dt)
+    else:
+        a, b, _, mu, _ = lanczos_build(apply, v1, m)
     return tridiag_eigvals(a, b)[:nev], a, b
 
 

@@ -386,6 +386,68 @@ orc_basis* orc_translational(int L, int base, int k, int N, int a, orc_pred f, v
   return b;
 }
 
+// The TranslationalBasis of given tables (I 1-based ascending, R), with the
+// phase table of TranslationalBasis.jl:264 / 277-285: for sectors too large to
+// scan here, whose tables the tests check by sampling (orc_trans_judge).
+orc_basis* orc_translational_tables(int L, int base, int k, int a, int64_t D, const int64_t* I,
+                                    const double* R) {
+  if (a <= 0 || L % a != 0) { g_err = "Length of unit-cell incompatible with L"; return nullptr; }
+  auto* b = new OBasis; b->kind = K_TRANS; b->L = L; b->base = base; b->A = a;
+  int len = L / a; b->len = len;
+  int K = ((-k) % len + len) % len;
+  b->I.assign(I, I + D);
+  b->R.assign(R, R + D);
+  b->C.resize(len);
+  const double twopi = 2.0 * M_PI;
+  for (int i = 0; i < len; ++i) {
+    if (K == 0) b->C[i] = 1.0;
+    else if (2 * K == len) b->C[i] = (i % 2 == 0) ? 1.0 : -1.0;
+    else {
+      double th = ((-twopi / (double)len) * (double)K) * (double)i;
+      if (i == 0) b->C[i] = cplx(1.0, th);
+      else b->C[i] = cplx(std::cos(th), std::sin(th));
+    }
+  }
+  return b;
+}
+
+// The TranslationalBasis judge (TranslationalBasis.jl:94-114, norms :251-255)
+// on explicit 1-based indices: accept[q] = 1 and R[q] = the norm when index
+// idx[q] is an orbit representative of the sector (charge N, momentum k),
+// else accept[q] = 0.  The same judge as orc_translational's scan.
+void orc_trans_judge(int L, int base, int k, int N, int a, int64_t n, const int64_t* idx,
+                     uint8_t* accept, double* R) {
+  int len = L / a;
+  int K = ((-k) % len + len) % len;
+  std::vector<double> norm(len);
+  for (int i = 1; i <= len; ++i) norm[i - 1] = (double)len / std::sqrt((double)i);
+#pragma omp parallel
+  {
+    std::vector<int64_t> dgt(L), tmp(L);
+#pragma omp for schedule(static)
+    for (int64_t q = 0; q < n; ++q) {
+      const int64_t i = idx[q];
+      change_dgt(dgt.data(), L, i, base);
+      accept[q] = 0;
+      R[q] = 0.0;
+      if (!charge_ok(dgt.data(), L, base, N)) continue;
+      double nrm = norm[len - 1];
+      bool ok = true;
+      for (int m = 1; m <= len - 1; ++m) {
+        circshift(dgt.data(), L, a, tmp.data());
+        int64_t In = index_dgt(dgt.data(), L, base);
+        if (In < i) { ok = false; break; }
+        if (In == i) {
+          if (((int64_t)m * K) % len != 0) ok = false;
+          else nrm = norm[m - 1];
+          break;
+        }
+      }
+      if (ok) { accept[q] = 1; R[q] = nrm; }
+    }
+  }
+}
+
 // TranslationParityBasis(; L, f, k, p, N, a, base) — TranslationalParityBasis.jl:141-175,
 // judge :68-112.
 orc_basis* orc_transparity(int L, int base, int k, int p, int N, int a, orc_pred f, void* ud,
@@ -783,6 +845,80 @@ void orc_mul_cols(const orc_operator* op, const double* x, double* y, int64_t nv
     for (int t = 1; t < nt; ++t) s += Ms[t][i];
     Y[i] = s;
   }
+}
+
+// Rows of H*x through columns: y[q] = sum_t conj(H[t, j]) x[t] for j = rows[q]
+// (1-based), the entries H[:, j] being exactly those colmn! scatters for
+// column j (Operator.jl:426-465: H[pos, j] = coefficient(index) * M[r, c] /
+// R[j]).  For a Hermitian operator this is row j of H*x; the tests use it to
+// check sampled rows of products whose full oracle mul would take too long.
+// x and y complex interleaved.
+void orc_rows_hermitian(const orc_operator* op, int64_t n, const int64_t* rows, const double* x,
+                        double* y) {
+  const OBasis& b = *op->b;
+  const cplx* X = reinterpret_cast<const cplx*>(x);
+  cplx* Y = reinterpret_cast<cplx*>(y);
+#pragma omp parallel
+  {
+    std::vector<int64_t> dgt(b.L);
+#pragma omp for schedule(dynamic, 16)
+    for (int64_t q = 0; q < n; ++q) {
+      const int64_t j = rows[q];
+      change_dgt(dgt.data(), b.L, basis_content(b, j), b.base);
+      const double r = basis_norm(b, j);
+      cplx acc(0.0, 0.0);
+      for (const OTerm& t : op->terms) {
+        int ns = (int)t.sites.size();
+        int64_t jl = index_sites(dgt.data(), t.sites.data(), ns, b.base);
+        bool change = false;
+        for (int64_t k = t.colptr[jl - 1]; k < t.colptr[jl]; ++k) {
+          change_sites(dgt.data(), t.sites.data(), ns, t.rowval[k - 1], b.base);
+          auto ci = basis_index(b, dgt.data());
+          if (ci.first != 0.0) acc += std::conj(ci.first * t.nzval[k - 1] / r) * X[ci.second - 1];
+          change = true;
+        }
+        if (change) change_sites(dgt.data(), t.sites.data(), ns, jl, b.base);
+      }
+      Y[q] = acc;
+    }
+  }
+}
+
+// The nonzeros colmn! scatters, as coordinate triplets (duplicates not
+// summed): entry (pos, j, H[pos, j]) with H[pos, j] = coefficient(index) *
+// M[r, c] / R[j] for every column j (Operator.jl:426-465), pos and j 1-based.
+// With rows == nullptr only the count is returned.
+int64_t orc_coo(const orc_operator* op, int64_t* rows, int64_t* cols, double* vals) {
+  const OBasis& b = *op->b;
+  const int64_t D = b.dim();
+  std::vector<int64_t> dgt(b.L);
+  int64_t n = 0;
+  for (int64_t j = 1; j <= D; ++j) {
+    change_dgt(dgt.data(), b.L, basis_content(b, j), b.base);
+    const double r = basis_norm(b, j);
+    for (const OTerm& t : op->terms) {
+      int ns = (int)t.sites.size();
+      int64_t jl = index_sites(dgt.data(), t.sites.data(), ns, b.base);
+      bool change = false;
+      for (int64_t k = t.colptr[jl - 1]; k < t.colptr[jl]; ++k) {
+        change_sites(dgt.data(), t.sites.data(), ns, t.rowval[k - 1], b.base);
+        auto ci = basis_index(b, dgt.data());
+        if (ci.first != 0.0) {
+          if (rows) {
+            const cplx h = ci.first * t.nzval[k - 1] / r;
+            rows[n] = ci.second;
+            cols[n] = j;
+            vals[2 * n] = h.real();
+            vals[2 * n + 1] = h.imag();
+          }
+          ++n;
+        }
+        change = true;
+      }
+      if (change) change_sites(dgt.data(), t.sites.data(), ns, jl, b.base);
+    }
+  }
+  return n;
 }
 
 // Array(opt) — Operator.jl:171-196: dense column-major D x D complex matrix
