@@ -2,13 +2,13 @@
 //
 // edk_basis_index with host pointers stages the states and the results in
 // device buffers it allocates for the call.  Some callers cannot allocate
-// device memory at the point where they need a lookup: code that runs while
-// a stream is being captured into a CUDA graph (an allocation there breaks
-// the capture), latency-sensitive loops that must not pay for the
-// allocator's implicit synchronisation, and host runtimes that call in from
-// contexts where they forbid allocation (for example a garbage collector's
-// finaliser or a callback that must not block).  edk_basis_index_noalloc
-// serves them from a fixed scratch area that is part of the library image.
+// device memory at the point where they need a lookup: host runtimes that
+// call in from contexts where they forbid allocation (for example a garbage
+// collector's finaliser or a callback that must not block), latency-sensitive
+// loops that must not pay for the allocator's implicit synchronisation, and
+// processes in which another component has already reserved all device
+// memory for its own pool.  edk_basis_index_noalloc serves them from a fixed
+// scratch area that is part of the library image.
 //
 // The scratch is a file-scope __device__ array of kNoAllocBytes (2 MiB): room
 // for kNoAllocMaxStates states with their positions and coefficients.  Every

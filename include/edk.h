@@ -2,8 +2,7 @@
  * edk.h — C ABI of libedk, the B200 (sm_100a) implementation of EDKit.jl's
  * matrix-free operator application and the Lanczos / Krylov loops built on it.
  *
- * A Julia host binds these with `ccall` (see the binding in INTEGRATION.md);
- * Python binds them with ctypes.  No CUDA or torch types cross this boundary:
+ * A Julia host binds these with `ccall`; Python binds them with ctypes.  No CUDA or torch types cross this boundary:
  * only plain pointers, sizes and the POD structs below.
  *
  * Conventions (identical to EDKit.jl):
@@ -120,11 +119,13 @@ edk_status edk_basis_index(const edk_basis* b, int64_t n, const uint64_t* states
  * results as edk_basis_index(..., EDK_HOST), staged through a fixed 2 MiB
  * scratch area inside the library (at most 65536 states per call; larger n is
  * rejected with EDK_INVALID_ARG).  For callers that cannot allocate device
- * memory where they need a lookup, such as code running during CUDA-graph
- * capture or host callbacks that forbid allocation.  The scratch address is
- * resolved on the first call for each device, so make that first call before
- * any stream capture; calls are serialised and synchronous.  This entry point
- * has no counterpart in the reference. */
+ * memory where they need a lookup, such as host callbacks that forbid
+ * allocation or processes whose device memory another component has already
+ * reserved.  The scratch address is resolved on the first call for each
+ * device, so make that first call before any stream capture; calls are
+ * serialised and synchronous, and work that another caller launched on the
+ * same scratch at the same time would race.  This entry point has no
+ * counterpart in the reference. */
 edk_status edk_basis_index_noalloc(const edk_basis* b, int64_t n, const uint64_t* states,
                                    int64_t* pos, double* coeff);
 

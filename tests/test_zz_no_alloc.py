@@ -1,7 +1,8 @@
 """edk_basis_index_noalloc: index() through the C ABI without device allocation.
 
-Callers that cannot allocate device memory at the point of a lookup (graph
-capture, allocation-free host callbacks) use this entry point; it must give
+Callers that cannot allocate device memory at the point of a lookup (host
+callbacks that forbid allocation, processes whose device memory another
+component has reserved) use this entry point; it must give
 exactly what edk_basis_index gives, call after call, from its shared fixed
 scratch.  This file is collected last so that a failure here leaves every
 other test already run."""
