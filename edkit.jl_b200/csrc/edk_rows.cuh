@@ -454,81 +454,6 @@ __device__ __forceinline__ Cx<typename VTraits<VT>::A> ff_row_sum(
         return st ^ (1u << p) ^ (1u << q);
       }
     };
-    if constexpr (RANKED) {
-      if (d == 1) {
-        // nearest-neighbour family on a rank table, software-pipelined: the
-        // table entries of the next pair of hits are requested before the psi
-        // gathers of the current pair, so the two dependent loads of a hit
-        // overlap with those of its neighbours.  The wrap-around hit (bit 0)
-        // comes first, alone, as in ascending bit order.
-        auto acc_hit = [&](uint32_t v, bool on, int p) {
-          constexpr uint32_t TM = FFTabSize<BK>::n - 1;
-          const bool ok = on && v != ~0u;
-          const int64_t pos = ok ? (int64_t)(v >> b.rank_shift) : 0;
-          const double2 c = t.coef[v & TM];
-          const Cx<A> x = ldv(xk + pos);
-          A tr = (A)c.x, ti = (A)c.y;
-          if (!same) {
-            if constexpr (CX) {
-              const double2 w = ((st >> p) & 1u) ? ff.v2[f] : ff.v1[f];
-              const A ur = fma_(-(A)w.y, ti, mul_((A)w.x, tr)), ui = fma_((A)w.y, tr, mul_((A)w.x, ti));
-              tr = ur;
-              ti = ui;
-            }
-          }
-          if (ok) {
-            if (same) acc_t<A, CX, CT>(S0, tr, ti, x);
-            else acc_t<A, CX, true>(S0, tr, ti, x);
-          }
-        };
-        if (bits & 1u) {
-          bits &= ~1u;
-          if (TPS == 1 || (pc++ % TPS) == sub) {
-            const uint32_t k = rkw != ~0u ? rkw : rank_after_swap(st, rs, 0, L - 1, t.binom);
-            acc_hit(__ldg(b.rankmap + k), true, 0);
-          }
-        }
-        auto next_pair = [&](int& p1, int& p2, bool& two) -> bool {
-          while (bits) {
-            p1 = __ffs(bits) - 1;
-            bits &= bits - 1;
-            two = bits != 0;
-            p2 = two ? __ffs(bits) - 1 : p1;
-            bits &= bits - 1;
-            if (TPS == 1 || (pc++ % TPS) == sub) return true;
-          }
-          return false;
-        };
-        auto entry = [&](int p) -> uint32_t {  // adjacent sites p - 1, p: rank change C(p-1, j)
-          const int a = p - 1;
-          const uint32_t e = t.binom[a * 33 + __popc(st & ((1u << a) - 1u))];
-          return __ldg(b.rankmap + (((st >> a) & 1u) ? rs + e : rs - e));
-        };
-        int p1 = 0, p2 = 0;
-        bool two = false;
-        bool have = next_pair(p1, p2, two);
-        uint32_t v1 = 0, v2 = 0;
-        if (have) {
-          v1 = entry(p1);
-          v2 = entry(p2);
-        }
-        while (have) {
-          int n1 = 0, n2 = 0;
-          bool ntwo = false;
-          const bool nhave = next_pair(n1, n2, ntwo);
-          uint32_t u1 = 0, u2 = 0;
-          if (nhave) {
-            u1 = entry(n1);
-            u2 = entry(n2);
-          }
-          acc_hit(v1, true, p1);
-          acc_hit(v2, two, p2);
-          v1 = u1; v2 = u2; p1 = n1; p2 = n2; two = ntwo; have = nhave;
-        }
-        fold_w<A, CX>(Y, same ? ff.v1[f] : make_double2(1.0, 0.0), S0);
-        continue;
-      }
-    }
     while (bits) {
       const int p1 = __ffs(bits) - 1;
       bits &= bits - 1;
