@@ -23,7 +23,6 @@
 #include <chrono>
 #include <cmath>
 #include <complex>
-#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -205,127 +204,6 @@ __global__ void __launch_bounds__(256) k_bdots(const BOp* __restrict__ ops,
       si += s_part[ww * ncols + c].y;
     }
     part[o.pofs + (int64_t)c * o.nchunk + chunk] = make_double2(sr, si);
-  }
-}
-
-// Column-wise dot products of one chunk (kChunk rows from r0): out[c * stride]
-// = sum_r conj(V[r0 + r, c]) w[r] for c < ncols, with the chunk's w in shared
-// memory; warp k takes the columns k, k + 8, ..., its lanes 32 rows apart, so
-// a column costs one warp reduction (not one per warp as in k_bdots).
-template <class VV, bool CX>
-__device__ __forceinline__ void dots_cols(const VV* __restrict__ Vr0, int64_t D, int nr, int ncols,
-                                          const double2* __restrict__ s_w,
-                                          double2* __restrict__ out, int64_t stride) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int c = warp; c < ncols; c += 8) {
-    const VV* Vc = Vr0 + (int64_t)c * D;
-    double ar = 0.0, ai = 0.0;
-#pragma unroll 8
-    for (int r = lane; r < kChunk; r += 32) {
-      if (r < nr) {
-        const double2 v = l2(Vc + r), x = s_w[r];
-        ar += v.x * x.x + v.y * x.y;
-        if (CX) ai += v.x * x.y - v.y * x.x;
-      }
-    }
-    ar = wsum(ar);
-    if (CX) ai = wsum(ai);
-    if (lane == 0) out[(int64_t)c * stride] = make_double2(ar, ai);
-  }
-}
-
-// part[pofs + c * nchunk + chunk] = sum_{rows of chunk} conj(V_q[r, c]) w_q[r]
-// (the column-wise form of k_bdots); blocks walk the chunks
-template <class VV, class WV>
-__global__ void __launch_bounds__(256) k_bdots_cols(const BOp* __restrict__ ops,
-                                                    const int* __restrict__ chunk2op,
-                                                    int64_t nchunks, const VV* __restrict__ V,
-                                                    const WV* __restrict__ w,
-                                                    double2* __restrict__ part,
-                                                    const int* __restrict__ step,
-                                                    const int* __restrict__ done) {
-  __shared__ double2 s_w[kChunk];
-  constexpr bool CX = IsCx<VV>::v || IsCx<WV>::v;
-  const int ncols = *step + 1;
-  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-    const int q = chunk2op[ch];
-    if (done[q]) continue;
-    const BOp& o = ops[q];
-    const int64_t chunk = ch - o.chunk0, r0 = chunk * kChunk;
-    const int nr = (int)min((int64_t)kChunk, o.D - r0);
-    __syncthreads();  // the previous chunk's readers of s_w are done
-    for (int t = threadIdx.x; t < kChunk; t += blockDim.x)
-      s_w[t] = t < nr ? l2(w + o.woff + r0 + t) : make_double2(0.0, 0.0);
-    __syncthreads();
-    dots_cols<VV, CX>(V + o.voff + r0, o.D, nr, ncols, s_w, part + o.pofs + chunk, o.nchunk);
-  }
-}
-
-// The first update and the second set of dot products in one pass over a
-// chunk: wout = win - V_q coef_q for the chunk's rows (thread per row, V read
-// from HBM), then part = V_q^H wout over the same rows (V read again while it
-// is still in L2: the grid is kept to one or two blocks per SM so that the
-// chunks in flight fit in L2).  The CGS2 step then reads V three times, not four.
-template <class VV, class WI, class WO>
-__global__ void __launch_bounds__(256) k_bupdate_dots(const BOp* __restrict__ ops,
-                                                      const int* __restrict__ chunk2op,
-                                                      int64_t nchunks, int ncap,
-                                                      const VV* __restrict__ V,
-                                                      const double2* __restrict__ coef,
-                                                      const WI* __restrict__ win,
-                                                      WO* __restrict__ wout,
-                                                      double2* __restrict__ part,
-                                                      const int* __restrict__ step,
-                                                      const int* __restrict__ done) {
-  extern __shared__ double2 s_dyn[];
-  double2* s_coef = s_dyn;          // ncap
-  double2* s_w = s_dyn + ncap;      // kChunk
-  constexpr bool CX = IsCx<VV>::v || IsCx<WI>::v;
-  const int ncols = *step + 1;
-  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-    const int q = chunk2op[ch];
-    if (done[q]) continue;
-    const BOp& o = ops[q];
-    const int64_t chunk = ch - o.chunk0, r0 = chunk * kChunk;
-    const int nr = (int)min((int64_t)kChunk, o.D - r0);
-    __syncthreads();
-    for (int c = threadIdx.x; c < ncols; c += blockDim.x) s_coef[c] = coef[(int64_t)q * ncap + c];
-    __syncthreads();
-    const VV* Vq = V + o.voff + r0;
-#pragma unroll
-    for (int k = 0; k < kChunk / 256; ++k) {
-      const int r = threadIdx.x + k * 256;
-      double2 acc = make_double2(0.0, 0.0);
-      if (r < nr) {
-        acc = l2(win + o.woff + r0 + r);
-        const VV* Vr = Vq + r;
-        int c = 0;
-        for (; c + 4 <= ncols; c += 4) {
-          const double2 v0 = l2(Vr + (int64_t)(c + 0) * o.D), v1 = l2(Vr + (int64_t)(c + 1) * o.D);
-          const double2 v2 = l2(Vr + (int64_t)(c + 2) * o.D), v3 = l2(Vr + (int64_t)(c + 3) * o.D);
-          const double2 k0 = s_coef[c], k1 = s_coef[c + 1], k2 = s_coef[c + 2], k3 = s_coef[c + 3];
-          acc.x -= v0.x * k0.x + v1.x * k1.x + v2.x * k2.x + v3.x * k3.x;
-          if (CX) {
-            acc.x += v0.y * k0.y + v1.y * k1.y + v2.y * k2.y + v3.y * k3.y;
-            acc.y -= v0.x * k0.y + v0.y * k0.x + v1.x * k1.y + v1.y * k1.x + v2.x * k2.y +
-                     v2.y * k2.x + v3.x * k3.y + v3.y * k3.x;
-          }
-        }
-        for (; c < ncols; ++c) {
-          const double2 v = l2(Vr + (int64_t)c * o.D), kk = s_coef[c];
-          acc.x -= v.x * kk.x;
-          if (CX) {
-            acc.x += v.y * kk.y;
-            acc.y -= v.x * kk.y + v.y * kk.x;
-          }
-        }
-        s2(wout + o.woff + r0 + r, acc);
-        acc = l2(wout + o.woff + r0 + r);  // the stored value (WO may round)
-      }
-      s_w[r] = acc;
-    }
-    __syncthreads();
-    dots_cols<VV, CX>(Vq, o.D, nr, ncols, s_w, part + o.pofs + chunk, o.nchunk);
   }
 }
 
@@ -637,27 +515,7 @@ struct BatchEngine {
       set_error("batch Lanczos: too many steps for the shared-memory reduction (max 1800)");
       return EDK_UNSUPPORTED;
     }
-    {
-      int dev = 0;
-      if (cudaGetDevice(&dev) == cudaSuccess)
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-      if (nsm < 1) nsm = 148;
-    }
-    const size_t fsm = (size_t)(ncap + kChunk) * sizeof(double2);
-    fused = fsm <= 227 * 1024;
-    if (const char* e = std::getenv("EDK_UNFUSED_CGS")) fused = fused && e[0] != '1';
     // large dynamic shared memory is opted into here, outside any capture
-    if (fused && fsm > 48 * 1024) {
-      EDK_RETURN_IF(with_vt(vdt, [&](auto vp) -> edk_status {
-        using VV = std::remove_pointer_t<decltype(vp)>;
-        return with_vt(wdt, [&](auto wp) -> edk_status {
-          using WD = std::remove_pointer_t<decltype(wp)>;
-          EDK_TRY_CUDA(cudaFuncSetAttribute(k_bupdate_dots<VV, VV, WD>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
-          return EDK_OK;
-        });
-      }));
-    }
     return with_vt(vdt, [&](auto vp) -> edk_status {
       using VV = std::remove_pointer_t<decltype(vp)>;
       return with_vt(wdt, [&](auto wp) -> edk_status {
@@ -758,37 +616,6 @@ struct BatchEngine {
     });
   }
 
-  int nsm = 148;
-  bool fused = false;  // update + dots in one pass (k_bupdate_dots) when its shared memory fits
-
-  template <class XT>
-  edk_status launch_dots_cols(const XT* x) {
-    return with_vt(vdt, [&](auto vp) -> edk_status {
-      using VV = std::remove_pointer_t<decltype(vp)>;
-      const unsigned g = (unsigned)std::min<int64_t>(nchunks, (int64_t)nsm * 8);
-      k_bdots_cols<VV, XT><<<g, 256, 0, st>>>(d_ops(), chunk2op.as<int>(), nchunks, V.as<VV>(), x,
-                                              part.as<double2>(), step.as<int>(), done.as<int>());
-      return EDK_OK;
-    });
-  }
-
-  template <class WI, class WO>
-  edk_status launch_update_dots(const double2* coef, const WI* win, WO* wout) {
-    const size_t smem = (size_t)(ncap + kChunk) * sizeof(double2);
-    return with_vt(vdt, [&](auto vp) -> edk_status {
-      using VV = std::remove_pointer_t<decltype(vp)>;
-      // one block per SM, two when the chunks in flight at half the steps fit in L2
-      const double window = 2.0 * nsm * kChunk * (ncap / 2.0) * sizeof(VV);
-      const int per = window <= 96.0 * (1 << 20) ? 2 : 1;
-      const unsigned g = (unsigned)std::min<int64_t>(nchunks, (int64_t)nsm * per);
-      k_bupdate_dots<VV, WI, WO><<<g, 256, smem, st>>>(d_ops(), chunk2op.as<int>(), nchunks, ncap,
-                                                       V.as<VV>(), coef, win, wout,
-                                                       part.as<double2>(), step.as<int>(),
-                                                       done.as<int>());
-      return EDK_OK;
-    });
-  }
-
   template <class WI, class WO>
   edk_status launch_update(const double2* coef, const WI* win, WO* wout, bool norm, int zero) {
     size_t smem = (size_t)ncap * sizeof(double2);
@@ -810,15 +637,11 @@ struct BatchEngine {
       using VV = std::remove_pointer_t<decltype(vp)>;
       return with_vt(wdt, [&](auto wp) -> edk_status {
         using WD = std::remove_pointer_t<decltype(wp)>;
-        EDK_RETURN_IF(launch_dots_cols<VV>(wt.as<VV>()));
+        EDK_RETURN_IF(launch_dots<VV>(wt.as<VV>()));
         k_breduce<<<nops, 256, 0, st>>>(d_ops(), ncap, part.as<double2>(), coef1.as<double2>(),
                                         step.as<int>(), done.as<int>());
-        if (fused) {
-          EDK_RETURN_IF((launch_update_dots<VV, WD>(coef1.as<double2>(), wt.as<VV>(), w.as<WD>())));
-        } else {
-          EDK_RETURN_IF((launch_update<VV, WD>(coef1.as<double2>(), wt.as<VV>(), w.as<WD>(), false, 0)));
-          EDK_RETURN_IF(launch_dots<WD>(w.as<WD>()));
-        }
+        EDK_RETURN_IF((launch_update<VV, WD>(coef1.as<double2>(), wt.as<VV>(), w.as<WD>(), false, 0)));
+        EDK_RETURN_IF(launch_dots<WD>(w.as<WD>()));
         k_breduce<<<nops, 256, 0, st>>>(d_ops(), ncap, part.as<double2>(), coef2.as<double2>(),
                                         step.as<int>(), done.as<int>());
         EDK_RETURN_IF((launch_update<WD, WD>(coef2.as<double2>(), w.as<WD>(), w.as<WD>(), true, 0)));
