@@ -64,7 +64,7 @@ __device__ __forceinline__ double wsum(double v) {
 }  // namespace
 
 // One operator of a batch, as the kernels see it.
-struct BOp {
+struct __align__(16) BOp {
   BasisDev b;
   OpDev op;
   FFParams ff;
@@ -97,20 +97,27 @@ __global__ void __launch_bounds__(256) k_bapply_ff(const BOp* __restrict__ ops,
 
 // the row-plan form of k_bapply_ff (rank-searched sectors whose operators all
 // carry a plan): tile t of operator q is window t of q's plan
-template <int BK, class VT>
-__global__ void __launch_bounds__(256) k_bapply_plan(const BOp* __restrict__ ops,
+template <int BK, class VT, int NN>
+__global__ void __launch_bounds__(256, plan_min_blocks<BK, VT>()) k_bapply_plan(const BOp* __restrict__ ops,
                                                      const int* __restrict__ tile2op,
                                                      const VT* __restrict__ V, VT* __restrict__ wt,
                                                      const int* __restrict__ step,
                                                      const int* __restrict__ done) {
   __shared__ FFTab<BK> sm;
+  __shared__ __align__(16) BOp s_op;  // the operator record, read from shared memory
   const int q = tile2op[blockIdx.x];
   if (done[q]) return;
-  const BOp& o = ops[q];
+  {
+    const int4* src = reinterpret_cast<const int4*>(ops + q);
+    int4* dst = reinterpret_cast<int4*>(&s_op);
+    for (int e = threadIdx.x; e < (int)(sizeof(BOp) / sizeof(int4)); e += blockDim.x) dst[e] = src[e];
+  }
+  __syncthreads();
+  const BOp& o = s_op;
   ff_tab_fill<BK>(sm, o.b, o.op.plan.binom);
   __syncthreads();
   const int j = *step;
-  plan_row<BK, VT>(o.b, o.op, o.ff, sm, (blockIdx.x - o.tile0) * (int64_t)kTile + threadIdx.x,
+  plan_row<BK, VT, NN>(o.b, o.op, o.ff, sm, (blockIdx.x - o.tile0) * (int64_t)kTile + threadIdx.x,
                    V + o.voff + (int64_t)j * o.D, wt + o.woff, 0);
 }
 
@@ -406,6 +413,7 @@ struct BatchEngine {
   int bk = 0;
   bool ff = false;
   bool plan = false;  // every operator carries a row plan (rank-searched sectors)
+  bool plan_nn_all = false;  // ... and is one nearest-neighbour family of equal values
   bool sell = false;
   int64_t nsblk = 0;
   cudaStream_t st = nullptr;
@@ -429,11 +437,13 @@ struct BatchEngine {
     // row plans (built here, outside any capture) when the sectors are ranked
     plan = use_ff && (lookup_kind == BK_TRANS0_RANK || lookup_kind == BK_TRANS_RANK ||
                       lookup_kind == BK_TRANSPAR_RANK || lookup_kind == BK_PROJ_RANK);
+    plan_nn_all = plan;
     for (auto* op : ops) {
       if (!plan) break;
       if (!plan_applies(op)) { plan = false; break; }
       EDK_RETURN_IF(plan_ensure(op));
       plan = op->plan_state == 1;
+      plan_nn_all = plan_nn_all && plan_nn(*reinterpret_cast<const FFParams*>(op->ff_params.data()));
     }
     vdt = vdtype;
     wdt = (vdt == EDK_C128 || vdt == EDK_C64) ? EDK_C128 : EDK_F64;
@@ -558,16 +568,28 @@ struct BatchEngine {
       if (plan) {
         switch (bk) {
           case BK_PROJ_RANK:
-            k_bapply_plan<BK_PROJ_RANK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+            if (plan_nn_all)
+              k_bapply_plan<BK_PROJ_RANK, VT, 1><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+            else
+              k_bapply_plan<BK_PROJ_RANK, VT, 2><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
             return EDK_OK;
           case BK_TRANS0_RANK:
-            k_bapply_plan<BK_TRANS0_RANK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+            if (plan_nn_all)
+              k_bapply_plan<BK_TRANS0_RANK, VT, 1><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+            else
+              k_bapply_plan<BK_TRANS0_RANK, VT, 2><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
             return EDK_OK;
           case BK_TRANS_RANK:
-            k_bapply_plan<BK_TRANS_RANK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+            if (plan_nn_all)
+              k_bapply_plan<BK_TRANS_RANK, VT, 1><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+            else
+              k_bapply_plan<BK_TRANS_RANK, VT, 2><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
             return EDK_OK;
           case BK_TRANSPAR_RANK:
-            k_bapply_plan<BK_TRANSPAR_RANK, VT><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+            if (plan_nn_all)
+              k_bapply_plan<BK_TRANSPAR_RANK, VT, 1><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+            else
+              k_bapply_plan<BK_TRANSPAR_RANK, VT, 2><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
             return EDK_OK;
         }
       }

@@ -86,16 +86,9 @@ __global__ void __launch_bounds__(256) k_plan_build(BasisDev b, OpDev op, FFPara
   if (want_diag) dg_o[slot] = dr;
 }
 
-// Resident blocks per SM asked of the compiler: the plan kernel is latency
-// bound, so real vectors are held to 32 registers (all 64 warp slots of an SM
-// filled), single-precision complex to 40 (48 warps, no spills); double
-// complex keeps the compiler's choice.
-template <int BK, class VT>
-constexpr int plan_min_blocks() {
-  return std::is_same<VT, double2>::value ? 1 : (std::is_same<VT, float2>::value ? 6 : 8);
-}
-
-template <int BK, class VT>
+// NN = 1: the operator is one nearest-neighbour family of equal exchange
+// values (its loop only); NN = 2: any other operator (the general loop only)
+template <int BK, class VT, int NN>
 __global__ void __launch_bounds__(256, plan_min_blocks<BK, VT>())
     k_apply_plan(BasisDev b, OpDev op, FFParams ff, const VT* __restrict__ x,
                  VT* __restrict__ y, int64_t ldx, int64_t ldy, int accumulate, int64_t slot0,
@@ -107,7 +100,7 @@ __global__ void __launch_bounds__(256, plan_min_blocks<BK, VT>())
   VT* yk = y + (int64_t)blockIdx.y * ldy;
   for (int64_t s = slot0 + (int64_t)blockIdx.x * kPlanWindow + threadIdx.x; s < slot1;
        s += (int64_t)gridDim.x * kPlanWindow)
-    plan_row<BK, VT>(b, op, ff, sm, s, xk, yk, accumulate);
+    plan_row<BK, VT, NN>(b, op, ff, sm, s, xk, yk, accumulate);
 }
 
 int sm_count() {
@@ -119,25 +112,34 @@ int sm_count() {
   return n[dev];
 }
 
-template <int BK, class VT>
-edk_status launch_plan_kind(const BasisDev& b, const OpDev& op, const FFParams& ff, const VT* X,
-                            VT* Y, int64_t nvec, int64_t ldx, int64_t ldy, int accumulate,
-                            cudaStream_t st, int64_t slot0, int64_t slot1) {
+template <int BK, class VT, int NN>
+edk_status launch_plan_nn(const BasisDev& b, const OpDev& op, const FFParams& ff, const VT* X,
+                          VT* Y, int64_t nvec, int64_t ldx, int64_t ldy, int accumulate,
+                          cudaStream_t st, int64_t slot0, int64_t slot1) {
   static int per_sm = 0;  // resident blocks per SM of this instantiation
   if (!per_sm) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply_plan<BK, VT>, kPlanWindow,
-                                                      0) != cudaSuccess || per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply_plan<BK, VT, NN>,
+                                                      kPlanWindow, 0) != cudaSuccess || per_sm < 1)
       per_sm = 1;
   }
   const int64_t nwin = (slot1 - slot0) / kPlanWindow;
   const unsigned gx = (unsigned)std::min<int64_t>(nwin, (int64_t)sm_count() * per_sm);
   for (int64_t k0 = 0; k0 < nvec; k0 += 65535) {
     const int64_t nk = std::min<int64_t>(nvec - k0, 65535);
-    k_apply_plan<BK, VT><<<dim3(gx, (unsigned)nk), kPlanWindow, 0, st>>>(
+    k_apply_plan<BK, VT, NN><<<dim3(gx, (unsigned)nk), kPlanWindow, 0, st>>>(
         b, op, ff, X + k0 * ldx, Y + k0 * ldy, ldx, ldy, accumulate, slot0, slot1);
     EDK_TRY_CUDA(cudaGetLastError());
   }
   return EDK_OK;
+}
+
+template <int BK, class VT>
+edk_status launch_plan_kind(const BasisDev& b, const OpDev& op, const FFParams& ff, const VT* X,
+                            VT* Y, int64_t nvec, int64_t ldx, int64_t ldy, int accumulate,
+                            cudaStream_t st, int64_t slot0, int64_t slot1) {
+  if (plan_nn(ff))
+    return launch_plan_nn<BK, VT, 1>(b, op, ff, X, Y, nvec, ldx, ldy, accumulate, st, slot0, slot1);
+  return launch_plan_nn<BK, VT, 2>(b, op, ff, X, Y, nvec, ldx, ldy, accumulate, st, slot0, slot1);
 }
 
 // lookup kind of the plan kernels for the basis as it is searched now, or -1

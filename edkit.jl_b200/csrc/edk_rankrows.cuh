@@ -21,14 +21,31 @@
 // wrap-around bond (its target rank is kept per slot).
 #pragma once
 
+#include <type_traits>
+
 #include "edk_rows.cuh"
 
 namespace edk {
 
+// Resident blocks per SM asked of the compiler: the plan kernels are latency
+// bound, so real vectors are held to 32 registers (all 64 warp slots of an SM
+// filled), single-precision complex to 40 (48 warps), double complex to 64
+// (32 warps).
+template <int BK, class VT>
+constexpr int plan_min_blocks() {
+  return std::is_same<VT, double2>::value ? 4 : (std::is_same<VT, float2>::value ? 6 : 8);
+}
+
+// The operator is one nearest-neighbour bond family with equal exchange
+// values (the plan kernels then compile only that loop: NN = 1; else NN = 2).
+__host__ __device__ inline bool plan_nn(const FFParams& ff) {
+  return ff.nfam == 1 && ff.d[0] == 1 && ff.same[0];
+}
+
 // One slot of the plan.  BK is BK_TRANS0_RANK, BK_TRANS_RANK,
 // BK_TRANSPAR_RANK (rank table) or BK_PROJ_RANK (row = rank); `t` holds the
 // block's tables (ff_tab_fill with the plan's binomials).
-template <int BK, class VT>
+template <int BK, class VT, int NN = 0>
 __device__ __forceinline__ void plan_row(const BasisDev& b, const OpDev& op, const FFParams& ff,
                                          const FFTab<BK>& t, int64_t slot,
                                          const VT* __restrict__ xk, VT* __restrict__ yk,
@@ -43,7 +60,7 @@ __device__ __forceinline__ void plan_row(const BasisDev& b, const OpDev& op, con
   const int64_t i = (int64_t)(rw & kPlanRowMask);
   // 1 / R of the row, rounded as the tile form rounds it (coef[c].x = R_c)
   const A invRi = BK == BK_PROJ_RANK ? (A)1 : (A)(1.0 / t.coef[rw >> 27].x);
-  const Cx<A> Y = ff_row_sum<BK, VT, 1>(b, ff, t, st, rs, rkw, 0, xk);
+  const Cx<A> Y = ff_row_sum<BK, VT, 1, NN>(b, ff, t, st, rs, rkw, 0, xk);
   double dr = 0.0, di = 0.0;
   if (pl.dg) {
     dr = __ldg(pl.dg + slot);  // the same sums, taken when the plan was built

@@ -421,7 +421,10 @@ __device__ __forceinline__ void ff_targets(const BasisDev& b, const FFTab<BK>& t
 // Off-diagonal sum of one row (before the factor 1/R_i).  TPS lanes share the
 // row and take its pairs of hits in turn (lane `sub`); rkw, when not ~0u, is
 // the precomputed rank of the state with bits 0 and L-1 exchanged.
-template <int BK, class VT, int TPS>
+// NN: 0 test at run time for the single nearest-neighbour family of equal
+// exchange values (and take its loop), 1 always take that loop (the caller
+// has checked), 2 never.
+template <int BK, class VT, int TPS, int NN = 0>
 __device__ __forceinline__ Cx<typename VTraits<VT>::A> ff_row_sum(
     const BasisDev& b, const FFParams& ff, const FFTab<BK>& t, uint32_t st, uint32_t rs,
     uint32_t rkw, int sub, const VT* __restrict__ xk) {
@@ -433,6 +436,72 @@ __device__ __forceinline__ Cx<typename VTraits<VT>::A> ff_row_sum(
   const uint32_t mask = (uint32_t)b.maskL;
   const int L = b.L;
   Cx<A> Y{0, 0};
+  if constexpr (BYRANK && TPS == 1 && NN != 2) {
+    // one nearest-neighbour family with equal exchange values (XXZ, Heisenberg
+    // chains): the same hits in the same order, without the per-hit tests of
+    // the general loop; the wrap-around hit (bit 0) first, then pairs
+    if (NN == 1 || (ff.nfam == 1 && ff.d[0] == 1 && ff.same[0])) {
+      uint32_t bits = (st ^ rotl_L(st, 1, L, mask)) & ff.valid[0];
+      Cx<A> S0{0, 0};
+      auto pair = [&](uint32_t k1, uint32_t k2, bool two) {
+        bool ok1, ok2;
+        int64_t pos1, pos2;
+        A t1r, t1i, t2r, t2i;
+        ff_targets<BK, A>(b, t, k1, k2, two, ok1, pos1, t1r, t1i, ok2, pos2, t2r, t2i);
+        const Cx<A> x1 = ldv(xk + pos1), x2 = ldv(xk + pos2);
+        if (ok1) acc_t<A, CX, CT>(S0, t1r, t1i, x1);
+        if (ok2) acc_t<A, CX, CT>(S0, t2r, t2i, x2);
+      };
+      auto adj = [&](int a) -> uint32_t {  // sites a, a + 1: rank change C(a, j)
+        const uint32_t e = t.binom[a * 33 + __popc(st & ((1u << a) - 1u))];
+        return ((st >> a) & 1u) ? rs + e : rs - e;
+      };
+      if (bits & 1u) {
+        bits &= ~1u;
+        const uint32_t k = rkw != ~0u ? rkw : rank_after_swap(st, rs, 0, L - 1, t.binom);
+        pair(k, k, false);
+      }
+      if constexpr (NN == 1) {  // four hits per pass: their table reads and psi gathers in flight together
+        while (bits) {
+          int p[4];
+          bool on[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            on[u] = bits != 0;
+            p[u] = on[u] ? __ffs(bits) - 1 : (u ? p[u - 1] : 1);
+            bits &= bits - 1;
+          }
+          uint32_t v[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) v[u] = __ldg(b.rankmap + adj(p[u] - 1));
+          constexpr uint32_t TM = FFTabSize<BK>::n - 1;
+          Cx<A> x[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            on[u] = on[u] && v[u] != ~0u;
+            x[u] = ldv(xk + (on[u] ? (int64_t)(v[u] >> b.rank_shift) : 0));
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const double2 c = t.coef[v[u] & TM];
+            if (on[u]) acc_t<A, CX, CT>(S0, (A)c.x, (A)c.y, x[u]);
+          }
+        }
+        fold_w<A, CX>(Y, ff.v1[0], S0);
+        return Y;
+      }
+      while (bits) {
+        const int p1 = __ffs(bits) - 1;
+        bits &= bits - 1;
+        const bool two = bits != 0;
+        const int p2 = two ? __ffs(bits) - 1 : p1;
+        bits &= bits - 1;
+        pair(adj(p1 - 1), adj(p2 - 1), two);
+      }
+      fold_w<A, CX>(Y, ff.v1[0], S0);
+      return Y;
+    }
+  }
   int pc = 0;  // pairs of hits seen so far in this row
   for (int f = 0; f < ff.nfam; ++f) {
     const int d = ff.d[f];
