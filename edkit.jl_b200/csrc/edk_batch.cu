@@ -214,29 +214,29 @@ __global__ void __launch_bounds__(256) k_bdots(const BOp* __restrict__ ops,
   }
 }
 
-// coef[q * ncap + c] = sum over the chunks of operator q (one block per operator)
+// coef[q * ncap + c] = sum over the chunks of operator q: block (x, q) sums
+// columns 8x .. 8x + 7 of operator q, one warp per column, so a large
+// operator's reduction is spread over many SMs
 __global__ void __launch_bounds__(256) k_breduce(const BOp* __restrict__ ops, int ncap,
                                                  const double2* __restrict__ part,
                                                  double2* __restrict__ coef,
                                                  const int* __restrict__ step,
                                                  const int* __restrict__ done) {
-  const int q = blockIdx.x;
-  if (done[q]) return;
+  const int q = blockIdx.y;
+  const int c = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (done[q] || c > *step) return;
+  const int lane = threadIdx.x & 31;
   const BOp& o = ops[q];
-  const int ncols = *step + 1;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int c = warp; c < ncols; c += 8) {
-    const double2* pc = part + o.pofs + (int64_t)c * o.nchunk;
-    double sr = 0.0, si = 0.0;
-    for (int k = lane; k < o.nchunk; k += 32) {
-      const double2 v = pc[k];
-      sr += v.x;
-      si += v.y;
-    }
-    sr = wsum(sr);
-    si = wsum(si);
-    if (lane == 0) coef[(int64_t)q * ncap + c] = make_double2(sr, si);
+  const double2* pc = part + o.pofs + (int64_t)c * o.nchunk;
+  double sr = 0.0, si = 0.0;
+  for (int k = lane; k < o.nchunk; k += 32) {
+    const double2 v = pc[k];
+    sr += v.x;
+    si += v.y;
   }
+  sr = wsum(sr);
+  si = wsum(si);
+  if (lane == 0) coef[(int64_t)q * ncap + c] = make_double2(sr, si);
 }
 
 // wout_q = win_q - V_q[:, 0:ncols] coef_q ; normpart[tile] = sum |wout|^2
@@ -434,6 +434,10 @@ struct BatchEngine {
   edk_status init(const std::vector<edk_operator*>& ops, int vdtype, int m_, int lookup_kind,
                   bool use_ff, cudaStream_t s) {
     nops = (int)ops.size();
+    if (nops > 65535) {
+      set_error("batch Lanczos: at most 65535 operators per batch");
+      return EDK_UNSUPPORTED;
+    }
     // row plans (built here, outside any capture) when the sectors are ranked
     plan = use_ff && (lookup_kind == BK_TRANS0_RANK || lookup_kind == BK_TRANS_RANK ||
                       lookup_kind == BK_TRANSPAR_RANK || lookup_kind == BK_PROJ_RANK);
@@ -660,11 +664,13 @@ struct BatchEngine {
       return with_vt(wdt, [&](auto wp) -> edk_status {
         using WD = std::remove_pointer_t<decltype(wp)>;
         EDK_RETURN_IF(launch_dots<VV>(wt.as<VV>()));
-        k_breduce<<<nops, 256, 0, st>>>(d_ops(), ncap, part.as<double2>(), coef1.as<double2>(),
+        k_breduce<<<dim3((ncap + 7) / 8, nops), 256, 0, st>>>(d_ops(), ncap, part.as<double2>(),
+                                                             coef1.as<double2>(),
                                         step.as<int>(), done.as<int>());
         EDK_RETURN_IF((launch_update<VV, WD>(coef1.as<double2>(), wt.as<VV>(), w.as<WD>(), false, 0)));
         EDK_RETURN_IF(launch_dots<WD>(w.as<WD>()));
-        k_breduce<<<nops, 256, 0, st>>>(d_ops(), ncap, part.as<double2>(), coef2.as<double2>(),
+        k_breduce<<<dim3((ncap + 7) / 8, nops), 256, 0, st>>>(d_ops(), ncap, part.as<double2>(),
+                                                             coef2.as<double2>(),
                                         step.as<int>(), done.as<int>());
         EDK_RETURN_IF((launch_update<WD, WD>(coef2.as<double2>(), w.as<WD>(), w.as<WD>(), true, 0)));
         k_bfinish<<<nops, 256, 0, st>>>(d_ops(), ncap, m, normpart.as<double>(),
