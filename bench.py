@@ -535,6 +535,8 @@ def config5_ensemble(ek, n_inst=512, seed=2024, steps=200):
                 ev[name], d = ek.batch_lanczos_e0(ops, v0s, m=steps, nev=nev, tol=1e-12,
                                                   check_every=10, **kw)
             r[name] = {"seconds": round(d["seconds"], 4), "max_steps": d["steps"],
+                       "max_steps_fp32": d["steps_low"], "seconds_stage1": round(d["seconds_stage1"], 4),
+                       "seconds_refine": round(d["seconds_refine"], 4),
                        "matvecs": d["matvecs"]}
         a, b = ev["fp64_batched"], ev["mixed_batched"]
         r["dE0_rel_max_mixed_vs_fp64"] = float(np.max(np.abs(b[:, 0] - a[:, 0]) / np.abs(a[:, 0])))
@@ -569,7 +571,9 @@ def config4_sectors(ek, steps=100, block=True):
     for name, kw in (("fp64_batched", {}), ("mixed_batched", {"precision": "mixed"})):
         for _ in range(2):
             ev, d = ek.batch_lanczos_e0(ops, m=300, nev=4, tol=1e-12, check_every=10, **kw)
-        res[name] = {"seconds": round(d["seconds"], 4), "max_steps": d["steps"]}
+        res[name] = {"seconds": round(d["seconds"], 4), "max_steps": d["steps"],
+                     "max_steps_fp32": d["steps_low"], "seconds_stage1": round(d["seconds_stage1"], 4),
+                     "seconds_refine": round(d["seconds_refine"], 4)}
         res[name + "_low4_k0"] = [float(v) for v in ev[0]]
         low[name] = ev
     res["E0_all_sectors"] = float(np.min(ev[:, 0]))
