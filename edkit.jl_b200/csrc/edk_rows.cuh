@@ -471,20 +471,34 @@ __device__ __forceinline__ Cx<typename VTraits<VT>::A> ff_row_sum(
             p[u] = on[u] ? __ffs(bits) - 1 : (u ? p[u - 1] : 1);
             bits &= bits - 1;
           }
+          // target ranks (a hit past the row's last one repeats the previous
+          // position: a valid rank whose product is not accumulated)
           uint32_t v[4];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) v[u] = __ldg(b.rankmap + adj(p[u] - 1));
-          constexpr uint32_t TM = FFTabSize<BK>::n - 1;
+          for (int u = 0; u < 4; ++u) v[u] = adj(p[u] - 1);
+          if constexpr (RANKED) {  // rank -> table entry (row, shift, class)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = __ldg(b.rankmap + v[u]);
+          }
           Cx<A> x[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            on[u] = on[u] && v[u] != ~0u;
-            x[u] = ldv(xk + (on[u] ? (int64_t)(v[u] >> b.rank_shift) : 0));
+            if constexpr (RANKED) {
+              on[u] = on[u] && v[u] != ~0u;
+              x[u] = ldv(xk + (on[u] ? (int64_t)(v[u] >> b.rank_shift) : 0));
+            } else {  // complete sector: the rank is the row
+              x[u] = ldv(xk + (int64_t)v[u]);
+            }
           }
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            const double2 c = t.coef[v[u] & TM];
-            if (on[u]) acc_t<A, CX, CT>(S0, (A)c.x, (A)c.y, x[u]);
+            if constexpr (RANKED) {
+              constexpr uint32_t TM = FFTabSize<BK>::n - 1;
+              const double2 c = t.coef[v[u] & TM];
+              if (on[u]) acc_t<A, CX, CT>(S0, (A)c.x, (A)c.y, x[u]);
+            } else {
+              if (on[u]) acc_t<A, CX, CT>(S0, (A)1, (A)0, x[u]);
+            }
           }
         }
         fold_w<A, CX>(Y, ff.v1[0], S0);
