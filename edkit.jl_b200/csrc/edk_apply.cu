@@ -291,7 +291,11 @@ edk_status apply_device(edk_operator* op, int dtype, const void* x, void* y, int
     EDK_TRY_CUDA(cudaMemset2DAsync(y, ldy * es, 0, b.D * es, nvec, st));
   }
   bool sc = !op->gather;
-  if (block_apply_ok(op, nvec) && (op->use_block > 0 || (op->use_block < 0 && !op->sell_ok)))
+  // automatic choice: the SpMM for a block of columns unless the operator is
+  // materialised or runs on a row plan (both stream one column faster than
+  // the SpMM locates hits once for all of them)
+  if (block_apply_ok(op, nvec) &&
+      (op->use_block > 0 || (op->use_block < 0 && !op->sell_ok && !plan_applies(op))))
     return apply_block(op, dtype, x, y, nvec, ldx, ldy, accumulate, st);
   if (op->sell_ok && !sc) return apply_sell(op, dtype, x, y, nvec, ldx, ldy, accumulate, st);
   if (op->ff_ok && !sc && op->use_ff) {

@@ -187,7 +187,40 @@ __global__ void __launch_bounds__(256) k_bdots(const BOp* __restrict__ ops,
     rows[k] = r0 + threadIdx.x + (int64_t)k * 256;
     wv[k] = rows[k] < D ? l2(wq + rows[k]) : make_double2(0.0, 0.0);
   }
-  for (int c = 0; c < ncols; ++c) {
+  // U columns per pass: their 4U loads in flight together, their U warp
+  // reductions interleaved
+  constexpr int U = CX ? 2 : 4;
+  int c = 0;
+  for (; c + U <= ncols; c += U) {
+    double ar[U], ai[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      ar[u] = 0.0;
+      ai[u] = 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const VV* Vc = Vq + (int64_t)(c + u) * D;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (rows[k] < D) {
+          const double2 v = l2(Vc + rows[k]);
+          ar[u] += v.x * wv[k].x + v.y * wv[k].y;
+          if (CX) ai[u] += v.x * wv[k].y - v.y * wv[k].x;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      ar[u] = wsum(ar[u]);
+      if (CX) ai[u] = wsum(ai[u]);
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) s_part[warp * ncols + c + u] = make_double2(ar[u], ai[u]);
+    }
+  }
+  for (; c < ncols; ++c) {
     const VV* Vc = Vq + (int64_t)c * D;
     double ar = 0.0, ai = 0.0;
 #pragma unroll

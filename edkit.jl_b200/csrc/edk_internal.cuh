@@ -330,7 +330,8 @@ struct edk_operator {
   int plan_state = 0;
   bool use_plan = true;   // tps == 1 on a rank-searched sector runs the plan kernel
   int use_block = -1;     // several right-hand sides through one SpMM: 1 yes, 0 no, -1 auto
-                          // (matrix-free yes, materialised no: its SpMV already streams)
+                          // (yes unless materialised or on a row plan, whose one-column
+                          // products already stream faster)
   std::vector<unsigned char> ff_params;
   int max_hits = 0;
   int nfam = 0, ngeneric = 0;

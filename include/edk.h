@@ -239,8 +239,8 @@ edk_status edk_block_lanczos(int32_t nops, edk_operator* const* ops,
  * right-hand sides as one SpMM on the bond-family and materialised paths
  * (each nonzero located once for all columns, as colmn! does,
  * Operator.jl:417-465); block = 0 runs them one column at a time; block = -1
- * (the default) uses the SpMM matrix-free and the columns on a materialised
- * matrix.  On a materialised operator, EDK_KERNEL_MATERIALIZED /
+ * (the default) uses the SpMM matrix-free, and the columns on a materialised
+ * matrix or a rank-searched sector (row-plan kernel).  On a materialised operator, EDK_KERNEL_MATERIALIZED /
  * EDK_KERNEL_MATERIALIZED_STAGED select its plain or shared-memory-staged
  * product (tps ignored).  Every
  * choice computes the same product as EDKit's mul! (Operator.jl:309-328).
