@@ -70,7 +70,7 @@ def measured_peak():
 
 def profiled_traffic(search="rank"):
     """dram bytes per launch of the matvec kernel from the committed ncu summary."""
-    name = "k_apply_ff_rank_L28_f64.md" if search == "rank" else "k_apply_trans0_L28_f64.md"
+    name = "k_apply_plan_rank_L28_f64.md" if search == "rank" else "k_apply_trans0_L28_f64.md"
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
