@@ -3,7 +3,8 @@
 // ground state as a batch of one.
 //
 // Every kernel of a step covers all operators of the batch in one launch: a
-// block owns a tile of one operator's rows (tile2op / chunk2op maps), reads
+// block owns a tile of one operator's rows (tile2op map) or, in the
+// reorthogonalisation kernels, an equal share of all rows (RowSplit), reads
 // that operator's basis/term descriptors from a device array, and works on
 // its slice of the concatenated buffers.  The step index j, the recurrence
 // coefficients alpha/beta, 1/beta and the per-operator stop flags live on the
@@ -12,8 +13,8 @@
 // steps (tridiagonal eigenvalues, convergence).  One step per operator q:
 //   wt_q = H_q v_j                       (row-gather matvec)
 //   s = V_q^H wt_q ; alpha_j = Re s_j     (CGS sweep 1, FP64 block partials)
-//   w_q = wt_q - V_q s
-//   u = V_q^H w_q ; w_q -= V_q u ; beta_j = ||w_q||   (sweep 2 + norm)
+//   w_q = wt_q - V_q s ; u = V_q^H w_q    (one pass: k_rupdate_dots)
+//   w_q -= V_q u ; beta_j = ||w_q||       (sweep 2 + norm)
 //   lucky breakdown beta <= sqrt(eps) max(1, |alpha|) stops operator q
 //   v_{j+1} = w_q / beta_j
 // (classical Gram-Schmidt twice, as _lanczos_build! in
@@ -35,7 +36,7 @@ namespace edk {
 namespace {
 
 constexpr int kTile = 256;          // rows per matvec / update tile
-constexpr int kChunk = 1024;        // rows per dots chunk (4 per thread)
+constexpr int kSplitBlocks = 4;         // resident reorthogonalisation blocks per SM (register cap)
 
 template <class T> struct IsCx;
 template <> struct IsCx<double> { static constexpr bool v = false; };
@@ -71,11 +72,9 @@ struct __align__(16) BOp {
   int64_t D;
   int64_t voff;   // element offset of V_q (D x ncap, column-major)
   int64_t woff;   // element offset into w / wt
-  int64_t pofs;   // offset of the dots partials (ncap x nchunk)
-  int64_t tile0;  // first matvec/update tile
-  int64_t chunk0; // first dots chunk
+  int64_t tile0;  // first matvec tile
   int64_t sblk0;  // first block of the materialised-matrix product (8 slices each)
-  int ntile, nchunk;
+  int ntile;
 };
 
 // ---------------------------------------------------------------------------
@@ -159,98 +158,259 @@ __global__ void __launch_bounds__(256) k_bapply_gen(const BOp* __restrict__ ops,
                                   s_binom);
 }
 
-// part[pofs + c * nchunk + chunk] = sum_{rows of chunk} conj(V_q[r, c]) w_q[r],  c <= j
+// Sum of eight values over a warp, one value index per lane group: three
+// halving exchanges (offsets 16, 8, 4: a lane keeps half of its values and
+// adds its partner's copy of that half) then two butterfly steps.  Nine
+// shuffles for eight sums instead of forty; lane l ends with the total of
+// value (l >> 2) & 7.
+__device__ __forceinline__ double wsum8(const double (&a)[8], int lane) {
+  double b[4], c[2];
+  const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double send = h16 ? a[i] : a[i + 4];
+    b[i] = (h16 ? a[i + 4] : a[i]) + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const double send = h8 ? b[i] : b[i + 2];
+    c[i] = (h8 ? b[i + 2] : b[i]) + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  double d = (h4 ? c[1] : c[0]) + __shfl_xor_sync(0xffffffffu, h4 ? c[0] : c[1], 4);
+  d += __shfl_xor_sync(0xffffffffu, d, 2);
+  d += __shfl_xor_sync(0xffffffffu, d, 1);
+  return d;
+}
+
+// ---------------------------------------------------------------------------
+// Reorthogonalisation kernels.  Their grid is G blocks that are all resident
+// at once (G = SMs x blocks per SM), and block b owns rows
+// [b T / G, (b + 1) T / G) of the concatenated rows of the operators still
+// running (T rows in all, recomputed by k_bsplit at the start of every step):
+// every block streams the same number of bytes, so no partly filled last
+// wave of blocks holds the launch up and operators that have stopped leave
+// no block idle.  A block whose rows run from one operator into the next
+// handles each piece in turn; its slot among operator q's partial sums is
+// b - bfirst_q (nslot_q slots in all).
+// ---------------------------------------------------------------------------
+struct SplitOp {
+  int64_t off;    // first row among the running operators' rows
+  int64_t pofs;   // offset of the dot-product partial sums (ncols x nslot)
+  int64_t slot0;  // first norm partial sum
+  int bfirst, nslot;
+};
+
+struct RowSplit {
+  const SplitOp* sp;
+  const int64_t* TG;  // rows of the running operators, blocks that share them
+  int nops;
+};
+
+// exclusive prefix sum over a block of 1024 threads; *total gets the sum
+__device__ int64_t block_scan1024(int64_t v, int64_t* s_warp, int64_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int64_t t = s_warp[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    s_warp[lane] = t;  // inclusive over warps
+  }
+  __syncthreads();
+  const int64_t before = (warp > 0 ? s_warp[warp - 1] : 0) + x - v;
+  *total = s_warp[31];
+  __syncthreads();
+  return before;
+}
+
+// the block holding row r: the largest b with b T / G <= r
+__device__ __forceinline__ int split_owner(int64_t r, int64_t T, int G) {
+  int64_t b = r * G / T;
+  while (b + 1 < G && (b + 1) * T / G <= r) ++b;
+  while (b > 0 && b * T / G > r) --b;
+  return (int)b;
+}
+
+// One block of 1024 threads: the running operators' row offsets, blocks and
+// partial-sum slots for this step.
+// The grid's first G' = min(G, ceil(T / 128)) blocks share the rows, so each
+// has at least one and every slot of an operator is written.
+__global__ void __launch_bounds__(1024) k_bsplit(const BOp* __restrict__ ops, int nops, int Gmax,
+                                                 int ncap, const int* __restrict__ done,
+                                                 SplitOp* __restrict__ sp, int64_t* __restrict__ TG) {
+  __shared__ int64_t s_warp[32];
+  const int per = (nops + 1023) / 1024;
+  const int q0 = min(nops, (int)threadIdx.x * per), q1 = min(nops, q0 + per);
+  int64_t loc = 0;
+  for (int q = q0; q < q1; ++q) loc += done[q] ? 0 : ops[q].D;
+  int64_t T = 0;
+  int64_t off = block_scan1024(loc, s_warp, &T);
+  const int G = (int)max((int64_t)1, min((int64_t)Gmax, (T + 127) / 128));
+  int64_t nsl = 0;
+  for (int q = q0; q < q1; ++q) {
+    const int64_t d = done[q] ? 0 : ops[q].D;
+    SplitOp o;
+    o.off = off;
+    o.pofs = 0;
+    o.slot0 = 0;
+    if (d > 0) {
+      o.bfirst = split_owner(off, T, G);
+      o.nslot = split_owner(off + d - 1, T, G) - o.bfirst + 1;
+    } else {
+      o.bfirst = 0;
+      o.nslot = 0;
+    }
+    sp[q] = o;
+    nsl += o.nslot;
+    off += d;
+  }
+  int64_t nslot_all = 0;
+  int64_t s0 = block_scan1024(nsl, s_warp, &nslot_all);
+  for (int q = q0; q < q1; ++q) {
+    sp[q].slot0 = s0;
+    sp[q].pofs = s0 * ncap;
+    s0 += sp[q].nslot;
+  }
+  if (threadIdx.x == 0) {
+    TG[0] = T;
+    TG[1] = G;
+  }
+}
+
+template <class F>
+__device__ __forceinline__ void for_block_rows(const BOp* __restrict__ ops, RowSplit rs, F&& f) {
+  const int64_t T = rs.TG[0], G = rs.TG[1];
+  if ((int64_t)blockIdx.x >= G) return;
+  const int64_t gb = (int64_t)blockIdx.x * T / G;
+  const int64_t ge = (int64_t)(blockIdx.x + 1) * T / G;
+  if (gb >= ge) return;
+  int lo = 0, hi = rs.nops - 1;  // the last operator starting at or before gb
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (rs.sp[mid].off <= gb) lo = mid;
+    else hi = mid - 1;
+  }
+  for (int q = lo; q < rs.nops; ++q) {
+    const SplitOp& s = rs.sp[q];
+    if (s.off >= ge) break;
+    if (s.nslot == 0) continue;  // stopped
+    const BOp& o = ops[q];
+    const int64_t a = max(gb, s.off), b = min(ge, s.off + o.D);
+    if (a < b) f(q, o, a - s.off, b - s.off, (int)blockIdx.x - s.bfirst, s);
+  }
+}
+
+// Rows per thread and pass of the reorthogonalisation kernels: a pass loads
+// U columns (8 real, 4 complex) of R rows in one go, 128 bytes a thread.
+template <class VV>
+constexpr int pass_rows() {
+  return 128 / ((IsCx<VV>::v ? 4 : 8) * (int)sizeof(VV));
+}
+
+// One pass of k_rdots: a += conj(V[rows, cols]) w[rows] for the U columns
+// at Vc[u] and the R rows rb + 256 k (all in range when FULL).
+template <bool FULL, int U, int R, bool CX, class VV, class WV>
+__device__ __forceinline__ void dots_pass(const VV* const (&Vc)[U], const WV* __restrict__ wq,
+                                          int64_t rb, int64_t r1, double (&a)[8]) {
+  double2 wv[R], v[U][R];
+#pragma unroll
+  for (int k = 0; k < R; ++k) {
+    const int64_t r = rb + (int64_t)k * 256;
+    wv[k] = (FULL || r < r1) ? l2(wq + r) : make_double2(0.0, 0.0);
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u)
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int64_t r = rb + (int64_t)k * 256;
+      v[u][k] = (FULL || r < r1) ? l2(Vc[u] + r) : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+  for (int u = 0; u < U; ++u)
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      if constexpr (CX) {
+        a[2 * u] += v[u][k].x * wv[k].x + v[u][k].y * wv[k].y;
+        a[2 * u + 1] += v[u][k].x * wv[k].y - v[u][k].y * wv[k].x;
+      } else {
+        a[u] += v[u][k].x * wv[k].x;
+      }
+    }
+}
+
+// part[pofs_q + c * nslot_q + slot] = sum over the block's rows r of
+// conj(V_q[r, c]) w_q[r], c <= j.  Columns go eight real (four complex)
+// values at a time through one wsum8 after the thread has summed its rows;
+// the columns of a last, partial group read the segment's last column again
+// (their sums are not kept).  The per-warp sums of 64 columns at a time are
+// added across warps in shared memory.
 template <class VV, class WV>
-__global__ void __launch_bounds__(256) k_bdots(const BOp* __restrict__ ops,
-                                               const int* __restrict__ chunk2op,
+__global__ void __launch_bounds__(256, kSplitBlocks) k_rdots(const BOp* __restrict__ ops, RowSplit rs,
                                                const VV* __restrict__ V,
                                                const WV* __restrict__ w,
                                                double2* __restrict__ part,
                                                const int* __restrict__ step,
                                                const int* __restrict__ done) {
-  extern __shared__ double2 s_part[];
   constexpr bool CX = IsCx<VV>::v || IsCx<WV>::v;
-  const int q = chunk2op[blockIdx.x];
-  if (done[q]) return;
-  const BOp& o = ops[q];
+  constexpr int U = CX ? 4 : 8;  // columns per reduction
+  constexpr int SEG = 64;        // columns per shared-memory flush
+  constexpr int R = pass_rows<VV>();
+  __shared__ double s_part[8][SEG][2];
   const int ncols = *step + 1;
-  const int64_t chunk = blockIdx.x - o.chunk0;
-  const int64_t r0 = chunk * kChunk;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t D = o.D;
-  const VV* Vq = V + o.voff;
-  const WV* wq = w + o.woff;
-  double2 wv[4];
-  int64_t rows[4];
+  for_block_rows(ops, rs, [&](int q, const BOp& o, int64_t r0, int64_t r1, int slot, const SplitOp& sq) {
+    if (done[q]) return;
+    const int64_t D = o.D;
+    const VV* Vq = V + o.voff;
+    const WV* wq = w + o.woff;
+    for (int s0 = 0; s0 < ncols; s0 += SEG) {
+      const int s1 = min(ncols, s0 + SEG);
+      for (int c = s0; c < s1; c += U) {
+        const VV* Vc[U];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    rows[k] = r0 + threadIdx.x + (int64_t)k * 256;
-    wv[k] = rows[k] < D ? l2(wq + rows[k]) : make_double2(0.0, 0.0);
-  }
-  // U columns per pass: their 4U loads in flight together, their U warp
-  // reductions interleaved
-  constexpr int U = CX ? 2 : 4;
-  int c = 0;
-  for (; c + U <= ncols; c += U) {
-    double ar[U], ai[U];
+        for (int u = 0; u < U; ++u) Vc[u] = Vq + (int64_t)min(c + u, s1 - 1) * D;
+        double a[8];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      ar[u] = 0.0;
-      ai[u] = 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const VV* Vc = Vq + (int64_t)(c + u) * D;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        if (rows[k] < D) {
-          const double2 v = l2(Vc + rows[k]);
-          ar[u] += v.x * wv[k].x + v.y * wv[k].y;
-          if (CX) ai[u] += v.x * wv[k].y - v.y * wv[k].x;
+        for (int u = 0; u < 8; ++u) a[u] = 0.0;
+        int64_t rb = r0 + threadIdx.x;
+        for (; rb + (int64_t)(R - 1) * 256 < r1; rb += 256 * R)
+          dots_pass<true, U, R, CX>(Vc, wq, rb, r1, a);
+        if (rb < r1) dots_pass<false, U, R, CX>(Vc, wq, rb, r1, a);
+        const double t = wsum8(a, lane);
+        if ((lane & 3) == 0) {
+          const int vi = lane >> 2;
+          const int col = CX ? c + (vi >> 1) : c + vi;
+          if (col < s1) s_part[warp][col - s0][CX ? (vi & 1) : 0] = t;
         }
       }
-    }
+      __syncthreads();
+      for (int c = threadIdx.x; c < s1 - s0; c += blockDim.x) {
+        double sr = 0.0, si = 0.0;
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      ar[u] = wsum(ar[u]);
-      if (CX) ai[u] = wsum(ai[u]);
-    }
-    if (lane == 0) {
-#pragma unroll
-      for (int u = 0; u < U; ++u) s_part[warp * ncols + c + u] = make_double2(ar[u], ai[u]);
-    }
-  }
-  for (; c < ncols; ++c) {
-    const VV* Vc = Vq + (int64_t)c * D;
-    double ar = 0.0, ai = 0.0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (rows[k] < D) {
-        const double2 v = l2(Vc + rows[k]);
-        ar += v.x * wv[k].x + v.y * wv[k].y;
-        if (CX) ai += v.x * wv[k].y - v.y * wv[k].x;
+        for (int ww = 0; ww < 8; ++ww) {
+          sr += s_part[ww][c][0];
+          if (CX) si += s_part[ww][c][1];
+        }
+        part[sq.pofs + (int64_t)(s0 + c) * sq.nslot + slot] = make_double2(sr, si);
       }
+      __syncthreads();
     }
-    ar = wsum(ar);
-    if (CX) ai = wsum(ai);
-    if (lane == 0) s_part[warp * ncols + c] = make_double2(ar, ai);
-  }
-  __syncthreads();
-  for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
-    double sr = 0.0, si = 0.0;
-#pragma unroll
-    for (int ww = 0; ww < 8; ++ww) {
-      sr += s_part[ww * ncols + c].x;
-      si += s_part[ww * ncols + c].y;
-    }
-    part[o.pofs + (int64_t)c * o.nchunk + chunk] = make_double2(sr, si);
-  }
+  });
 }
 
-// coef[q * ncap + c] = sum over the chunks of operator q: block (x, q) sums
-// columns 8x .. 8x + 7 of operator q, one warp per column, so a large
-// operator's reduction is spread over many SMs
-__global__ void __launch_bounds__(256) k_breduce(const BOp* __restrict__ ops, int ncap,
+// coef[q * ncap + c] = sum of operator q's slots: block (x, q) sums columns
+// 8x .. 8x + 7 of operator q, one warp per column
+__global__ void __launch_bounds__(256) k_breduce(const SplitOp* __restrict__ sp, int ncap,
                                                  const double2* __restrict__ part,
                                                  double2* __restrict__ coef,
                                                  const int* __restrict__ step,
@@ -259,10 +419,10 @@ __global__ void __launch_bounds__(256) k_breduce(const BOp* __restrict__ ops, in
   const int c = blockIdx.x * 8 + (threadIdx.x >> 5);
   if (done[q] || c > *step) return;
   const int lane = threadIdx.x & 31;
-  const BOp& o = ops[q];
-  const double2* pc = part + o.pofs + (int64_t)c * o.nchunk;
+  const SplitOp& o = sp[q];
+  const double2* pc = part + o.pofs + (int64_t)c * o.nslot;
   double sr = 0.0, si = 0.0;
-  for (int k = lane; k < o.nchunk; k += 32) {
+  for (int k = lane; k < o.nslot; k += 32) {
     const double2 v = pc[k];
     sr += v.x;
     si += v.y;
@@ -272,68 +432,195 @@ __global__ void __launch_bounds__(256) k_breduce(const BOp* __restrict__ ops, in
   if (lane == 0) coef[(int64_t)q * ncap + c] = make_double2(sr, si);
 }
 
-// wout_q = win_q - V_q[:, 0:ncols] coef_q ; normpart[tile] = sum |wout|^2
-// ncols = *step + 1 (or 0 with zero_cols)
+// acc[k] -= V[rows, cols] coef[cols] for the U columns at Vc[u] (coefficient
+// zero past the last column) and the R rows rb + 256 k (all in range when
+// FULL).
+template <bool FULL, int U, int R, bool CX, class VV>
+__device__ __forceinline__ void update_pass(const VV* const (&Vc)[U], const double2* kc,
+                                            int64_t rb, int64_t r1, double2 (&acc)[R]) {
+  double2 v[U][R];
+#pragma unroll
+  for (int u = 0; u < U; ++u)
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int64_t r = rb + (int64_t)k * 256;
+      v[u][k] = (FULL || r < r1) ? l2(Vc[u] + r) : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const double2 cu = kc[u];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      acc[k].x -= v[u][k].x * cu.x;
+      if (CX) {
+        acc[k].x += v[u][k].y * cu.y;
+        acc[k].y -= v[u][k].x * cu.y + v[u][k].y * cu.x;
+      }
+    }
+  }
+}
+
+// wout_q = win_q - V_q[:, 0:ncols] coef_q over the block's rows;
+// normpart[slot0_q + slot] = sum |wout|^2 over them.  ncols = *step + 1 (or 0
+// with zero_cols).  Columns go U at a time (the coefficients are padded with
+// zeros to a multiple of U, the missing columns read the last one again).
 template <class VV, class WI, class WO>
-__global__ void __launch_bounds__(256) k_bupdate(const BOp* __restrict__ ops,
-                                                 const int* __restrict__ tile2op, int ncap,
-                                                 const VV* __restrict__ V,
+__global__ void __launch_bounds__(256, kSplitBlocks) k_rupdate(const BOp* __restrict__ ops, RowSplit rs,
+                                                 int ncap, const VV* __restrict__ V,
                                                  const double2* __restrict__ coef,
                                                  const WI* __restrict__ win, WO* __restrict__ wout,
                                                  double* __restrict__ normpart,
                                                  const int* __restrict__ step,
                                                  const int* __restrict__ done, int zero_cols) {
-  extern __shared__ double2 s_coef[];
+  extern __shared__ double2 s_coef[];  // ncap + 8
+  __shared__ double s_n[8];
   constexpr bool CX = IsCx<VV>::v || IsCx<WI>::v;
-  const int q = tile2op[blockIdx.x];
-  if (done[q]) return;
-  const BOp& o = ops[q];
+  constexpr int U = CX ? 4 : 8;
+  constexpr int R = pass_rows<VV>();
   const int ncols = zero_cols ? 0 : *step + 1;
-  for (int c = threadIdx.x; c < ncols; c += blockDim.x) s_coef[c] = coef[(int64_t)q * ncap + c];
-  __syncthreads();
-  const int64_t r = (blockIdx.x - o.tile0) * (int64_t)kTile + threadIdx.x;
-  double nrm = 0.0;
-  if (r < o.D) {
-    const VV* Vq = V + o.voff + r;
-    double2 acc = l2(win + o.woff + r);
-    int c = 0;
-    for (; c + 4 <= ncols; c += 4) {
-      const double2 v0 = l2(Vq + (int64_t)(c + 0) * o.D), v1 = l2(Vq + (int64_t)(c + 1) * o.D);
-      const double2 v2 = l2(Vq + (int64_t)(c + 2) * o.D), v3 = l2(Vq + (int64_t)(c + 3) * o.D);
-      const double2 k0 = s_coef[c], k1 = s_coef[c + 1], k2 = s_coef[c + 2], k3 = s_coef[c + 3];
-      acc.x -= v0.x * k0.x + v1.x * k1.x + v2.x * k2.x + v3.x * k3.x;
-      if (CX) {
-        acc.x += v0.y * k0.y + v1.y * k1.y + v2.y * k2.y + v3.y * k3.y;
-        acc.y -= v0.x * k0.y + v0.y * k0.x + v1.x * k1.y + v1.y * k1.x + v2.x * k2.y +
-                 v2.y * k2.x + v3.x * k3.y + v3.y * k3.x;
-      }
-    }
-    for (; c < ncols; ++c) {
-      const double2 v = l2(Vq + (int64_t)c * o.D), k = s_coef[c];
-      acc.x -= v.x * k.x;
-      if (CX) {
-        acc.x += v.y * k.y;
-        acc.y -= v.x * k.y + v.y * k.x;
-      }
-    }
-    s2(wout + o.woff + r, acc);
-    nrm = acc.x * acc.x + (CX ? acc.y * acc.y : 0.0);
-  }
-  if (normpart) {
-    __shared__ double s_n[8];
-    nrm = wsum(nrm);
-    if ((threadIdx.x & 31) == 0) s_n[threadIdx.x >> 5] = nrm;
+  const int npad = (ncols + U - 1) / U * U;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for_block_rows(ops, rs, [&](int q, const BOp& o, int64_t r0, int64_t r1, int slot, const SplitOp& sq) {
+    if (done[q]) return;
+    __syncthreads();  // the previous piece's coefficients and norms are read
+    for (int c = threadIdx.x; c < npad; c += blockDim.x)
+      s_coef[c] = c < ncols ? coef[(int64_t)q * ncap + c] : make_double2(0.0, 0.0);
     __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int k = 0; k < 8; ++k) t += s_n[k];
-      normpart[blockIdx.x] = t;
+    const int64_t D = o.D;
+    const VV* Vq = V + o.voff;
+    double nrm = 0.0;
+    for (int64_t rb = r0 + threadIdx.x; rb < r1; rb += 256 * R) {
+      const bool full = rb + (int64_t)(R - 1) * 256 < r1;
+      double2 acc[R];
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        const int64_t r = rb + (int64_t)k * 256;
+        acc[k] = r < r1 ? l2(win + o.woff + r) : make_double2(0.0, 0.0);
+      }
+      for (int c = 0; c < npad; c += U) {
+        const VV* Vc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) Vc[u] = Vq + (int64_t)min(c + u, ncols - 1) * D;
+        if (full) update_pass<true, U, R, CX>(Vc, s_coef + c, rb, r1, acc);
+        else update_pass<false, U, R, CX>(Vc, s_coef + c, rb, r1, acc);
+      }
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        const int64_t r = rb + (int64_t)k * 256;
+        if (r < r1) {
+          s2(wout + o.woff + r, acc[k]);
+          nrm += acc[k].x * acc[k].x + (CX ? acc[k].y * acc[k].y : 0.0);
+        }
+      }
     }
-  }
+    if (normpart) {
+      nrm = wsum(nrm);
+      if (lane == 0) s_n[warp] = nrm;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < 8; ++k) t += s_n[k];
+        normpart[sq.slot0 + slot] = t;
+      }
+    }
+  });
+}
+
+// The first sweep's update and the second sweep's dot products in one pass,
+// 256 rows (one per thread) at a time: wout_q = win_q - V_q[:, 0:ncols]
+// coef_q, then, with the result still in registers, its dot products with
+// the same rows of every column, added per warp into shared memory; at the
+// end of the piece the warps' sums go to part[pofs_q + c * nslot_q + slot].
+// The dot products walk the columns in reverse, so the ones the update read
+// last, the most likely to be still in L2, are read again first.
+// Shared memory: ncap + 8 coefficients and 8 x ncap per-warp sums (double2).
+template <class VV, class WI, class WO>
+__global__ void __launch_bounds__(256, kSplitBlocks) k_rupdate_dots(const BOp* __restrict__ ops, RowSplit rs,
+                                                      int ncap, const VV* __restrict__ V,
+                                                      const double2* __restrict__ coef,
+                                                      const WI* __restrict__ win,
+                                                      WO* __restrict__ wout,
+                                                      double2* __restrict__ part,
+                                                      const int* __restrict__ step,
+                                                      const int* __restrict__ done) {
+  extern __shared__ double2 s_dyn[];
+  double2* s_coef = s_dyn;
+  double2* s_acc = s_dyn + ncap + 8;
+  constexpr bool CX = IsCx<VV>::v || IsCx<WI>::v || IsCx<WO>::v;
+  constexpr int U = CX ? 4 : 8;
+  const int ncols = *step + 1;
+  const int npad = (ncols + U - 1) / U * U;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for_block_rows(ops, rs, [&](int q, const BOp& o, int64_t r0, int64_t r1, int slot, const SplitOp& sq) {
+    if (done[q]) return;
+    __syncthreads();  // the previous piece's shared sums are written out
+    for (int c = threadIdx.x; c < npad; c += blockDim.x)
+      s_coef[c] = c < ncols ? coef[(int64_t)q * ncap + c] : make_double2(0.0, 0.0);
+    for (int i = threadIdx.x; i < 8 * ncols; i += blockDim.x)
+      s_acc[(i / ncols) * ncap + i % ncols] = make_double2(0.0, 0.0);
+    __syncthreads();
+    const int64_t D = o.D;
+    const VV* Vq = V + o.voff;
+    for (int64_t rb = r0; rb < r1; rb += 256) {
+      const int64_t r = rb + threadIdx.x;
+      const bool on = r < r1;
+      double2 acc[1] = {on ? l2(win + o.woff + r) : make_double2(0.0, 0.0)};
+      if (on) {
+        for (int c = 0; c < npad; c += U) {
+          const VV* Vc[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) Vc[u] = Vq + (int64_t)min(c + u, ncols - 1) * D;
+          update_pass<true, U, 1, CX>(Vc, s_coef + c, r, r + 1, acc);
+        }
+        WO t;
+        s2(&t, acc[0]);
+        wout[o.woff + r] = t;
+        acc[0] = l2(&t);  // the dot products see the stored value
+      }
+      for (int c = npad - U; c >= 0; c -= U) {
+        const VV* Vc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) Vc[u] = Vq + (int64_t)min(c + u, ncols - 1) * D + r;
+        double a[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) a[u] = 0.0;
+        if (on) {
+          double2 v[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) v[u] = l2(Vc[u]);
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            if constexpr (CX) {
+              a[2 * u] = v[u].x * acc[0].x + v[u].y * acc[0].y;
+              a[2 * u + 1] = v[u].x * acc[0].y - v[u].y * acc[0].x;
+            } else {
+              a[u] = v[u].x * acc[0].x;
+            }
+          }
+        }
+        const double t = wsum8(a, lane);
+        if ((lane & 3) == 0) {
+          const int vi = lane >> 2;
+          const int col = CX ? c + (vi >> 1) : c + vi;
+          if (col < ncols) reinterpret_cast<double*>(s_acc + warp * ncap + col)[CX ? (vi & 1) : 0] += t;
+        }
+      }
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+      double sr = 0.0, si = 0.0;
+#pragma unroll
+      for (int ww = 0; ww < 8; ++ww) {
+        sr += s_acc[ww * ncap + c].x;
+        si += s_acc[ww * ncap + c].y;
+      }
+      part[sq.pofs + (int64_t)c * sq.nslot + slot] = make_double2(sr, si);
+    }
+  });
 }
 
 // per operator: alpha_j, beta_j, breakdown, 1/beta (one block per operator)
-__global__ void __launch_bounds__(256) k_bfinish(const BOp* __restrict__ ops, int ncap, int m,
+__global__ void __launch_bounds__(256) k_bfinish(const SplitOp* __restrict__ sp, int ncap, int m,
                                                  const double* __restrict__ normpart,
                                                  const double2* __restrict__ coef1,
                                                  double* __restrict__ alpha,
@@ -344,9 +631,9 @@ __global__ void __launch_bounds__(256) k_bfinish(const BOp* __restrict__ ops, in
                                                  int* __restrict__ done, int setup) {
   const int q = blockIdx.x;
   if (done[q]) return;
-  const BOp& o = ops[q];
+  const SplitOp& o = sp[q];
   double s = 0.0;
-  for (int k = threadIdx.x; k < o.ntile; k += blockDim.x) s += normpart[o.tile0 + k];
+  for (int k = threadIdx.x; k < o.nslot; k += blockDim.x) s += normpart[o.slot0 + k];
   __shared__ double sh[8];
   s = wsum(s);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
@@ -452,8 +739,10 @@ struct BatchEngine {
   cudaStream_t st = nullptr;
   std::vector<BOp> hops;
   std::vector<int64_t> Ds;
-  int64_t ntiles = 0, nchunks = 0, totalD = 0;
-  DevBuf dops, tile2op, chunk2op, sblk2op, V, w, wt, part, coef1, coef2, normpart, alpha, beta, invb,
+  int64_t ntiles = 0, totalD = 0;
+  int G = 1;             // blocks of the reorthogonalisation grid
+  bool fused = false;    // first update and second dot products in one kernel
+  DevBuf dops, tile2op, sblk2op, splitops, splitT, V, w, wt, part, coef1, coef2, normpart, alpha, beta, invb,
       done, step, nsteps, cbuf, cnc;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -489,8 +778,8 @@ struct BatchEngine {
     bk = lookup_kind;
     ff = use_ff;
     st = s;
-    std::vector<int> t2o, c2o, s2o;
-    int64_t voff = 0, woff = 0, pofs = 0;
+    std::vector<int> t2o, s2o;
+    int64_t voff = 0, woff = 0;
     sell = true;
     for (auto* op : ops) sell = sell && op->sell_ok;
     for (int q = 0; q < nops; ++q) {
@@ -502,12 +791,9 @@ struct BatchEngine {
       if (use_ff) std::memcpy(&o.ff, op->ff_params.data(), sizeof(FFParams));
       o.D = op->b->D;
       o.ntile = (int)((o.D + kTile - 1) / kTile);
-      o.nchunk = (int)((o.D + kChunk - 1) / kChunk);
       o.voff = voff;
       o.woff = woff;
-      o.pofs = pofs;
       o.tile0 = ntiles;
-      o.chunk0 = nchunks;
       o.sblk0 = nsblk;
       if (sell) {
         const int64_t nb = (op->dev.sell.nslices + 7) / 8;
@@ -515,36 +801,35 @@ struct BatchEngine {
         nsblk += nb;
       }
       for (int k = 0; k < o.ntile; ++k) t2o.push_back(q);
-      for (int k = 0; k < o.nchunk; ++k) c2o.push_back(q);
       ntiles += o.ntile;
-      nchunks += o.nchunk;
       voff += o.D * ncap;
       woff += o.D;
-      pofs += (int64_t)o.nchunk * ncap;
       hops.push_back(o);
       Ds.push_back(o.D);
     }
     totalD = woff;
+    EDK_RETURN_IF(split_rows());
     EDK_RETURN_IF(dops.alloc_async(hops.size() * sizeof(BOp), st));
     EDK_TRY_CUDA(cudaMemcpyAsync(dops.p, hops.data(), hops.size() * sizeof(BOp),
                                  cudaMemcpyHostToDevice, st));
     EDK_RETURN_IF(tile2op.alloc_async(t2o.size() * 4, st));
     EDK_TRY_CUDA(cudaMemcpyAsync(tile2op.p, t2o.data(), t2o.size() * 4, cudaMemcpyHostToDevice, st));
-    EDK_RETURN_IF(chunk2op.alloc_async(c2o.size() * 4, st));
     if (sell) {
       EDK_RETURN_IF(sblk2op.alloc_async(std::max<size_t>(s2o.size(), 1) * 4, st));
       if (!s2o.empty())
         EDK_TRY_CUDA(cudaMemcpyAsync(sblk2op.p, s2o.data(), s2o.size() * 4,
                                      cudaMemcpyHostToDevice, st));
     }
-    EDK_TRY_CUDA(cudaMemcpyAsync(chunk2op.p, c2o.data(), c2o.size() * 4, cudaMemcpyHostToDevice, st));
     EDK_RETURN_IF(V.alloc_async((size_t)voff * esz(vdt), st));
     EDK_RETURN_IF(w.alloc_async((size_t)totalD * esz(wdt), st));
     EDK_RETURN_IF(wt.alloc_async((size_t)totalD * esz(vdt), st));
-    EDK_RETURN_IF(part.alloc_async((size_t)std::max<int64_t>(pofs, 1) * sizeof(double2), st));
+    // a block meets at most one operator more than it starts in: G + nops slots
+    EDK_RETURN_IF(part.alloc_async((size_t)(G + nops) * ncap * sizeof(double2), st));
+    EDK_RETURN_IF(splitops.alloc_async((size_t)nops * sizeof(SplitOp), st));
+    EDK_RETURN_IF(splitT.alloc_async(2 * sizeof(int64_t), st));
     EDK_RETURN_IF(coef1.alloc_async((size_t)nops * ncap * sizeof(double2), st));
     EDK_RETURN_IF(coef2.alloc_async((size_t)nops * ncap * sizeof(double2), st));
-    EDK_RETURN_IF(normpart.alloc_async((size_t)ntiles * sizeof(double), st));
+    EDK_RETURN_IF(normpart.alloc_async((size_t)(G + nops) * sizeof(double), st));
     EDK_RETURN_IF(alpha.alloc_async((size_t)nops * m * sizeof(double), st));
     EDK_RETURN_IF(beta.alloc_async((size_t)nops * m * sizeof(double), st));
     EDK_RETURN_IF(invb.alloc_async((size_t)nops * sizeof(double), st));
@@ -557,33 +842,53 @@ struct BatchEngine {
     EDK_TRY_CUDA(cudaMemsetAsync(nsteps.p, 0, nops * sizeof(int), st));
     EDK_TRY_CUDA(cudaMemsetAsync(alpha.p, 0, (size_t)nops * m * sizeof(double), st));
     EDK_TRY_CUDA(cudaMemsetAsync(beta.p, 0, (size_t)nops * m * sizeof(double), st));
-    size_t dsm = (size_t)8 * ncap * sizeof(double2);
-    if (dsm > 227 * 1024) {
-      set_error("batch Lanczos: too many steps for the shared-memory reduction (max 1800)");
+    return EDK_OK;
+  }
+
+  // Opt the reorthogonalisation kernels into the shared memory they need
+  // (outside any capture) and size their grid to what is resident at once.
+  edk_status split_rows() {
+    const size_t us = (size_t)(ncap + 8) * sizeof(double2);
+    if (us > 200 * 1024) {
+      set_error("batch Lanczos: too many steps for the shared-memory coefficients (max 12800)");
       return EDK_UNSUPPORTED;
     }
-    // large dynamic shared memory is opted into here, outside any capture
-    return with_vt(vdt, [&](auto vp) -> edk_status {
+    const size_t fs = us + (size_t)8 * ncap * sizeof(double2);  // + per-warp sums
+    fused = fs <= 200 * 1024;
+    int dev = 0, nsm = 0;
+    EDK_TRY_CUDA(cudaGetDevice(&dev));
+    EDK_TRY_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    int per_sm = 0;
+    edk_status s = with_vt(vdt, [&](auto vp) -> edk_status {
       using VV = std::remove_pointer_t<decltype(vp)>;
       return with_vt(wdt, [&](auto wp) -> edk_status {
         using WD = std::remove_pointer_t<decltype(wp)>;
-        const size_t us = (size_t)ncap * sizeof(double2);
-        const auto kd1 = k_bdots<VV, VV>;
-        const auto kd2 = k_bdots<VV, WD>;
-        const auto ku1 = k_bupdate<VV, VV, WD>;
-        const auto ku2 = k_bupdate<VV, WD, WD>;
         const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-        if (dsm > 48 * 1024) {
-          EDK_TRY_CUDA(cudaFuncSetAttribute(kd1, attr, (int)dsm));
-          EDK_TRY_CUDA(cudaFuncSetAttribute(kd2, attr, (int)dsm));
-        }
+        const auto ku1 = k_rupdate<VV, VV, WD>;
+        const auto ku2 = k_rupdate<VV, WD, WD>;
+        const auto kd1 = k_rdots<VV, VV>;
+        const auto kd2 = k_rdots<VV, WD>;
+        const auto kf = k_rupdate_dots<VV, VV, WD>;
         if (us > 48 * 1024) {
           EDK_TRY_CUDA(cudaFuncSetAttribute(ku1, attr, (int)us));
           EDK_TRY_CUDA(cudaFuncSetAttribute(ku2, attr, (int)us));
         }
+        if (fused && fs > 48 * 1024) EDK_TRY_CUDA(cudaFuncSetAttribute(kf, attr, (int)fs));
+        int n[5] = {0, 0, 0, 0, 0};
+        EDK_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[0], ku1, 256, us));
+        EDK_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[1], ku2, 256, us));
+        EDK_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[2], kd1, 256, 0));
+        EDK_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[3], kd2, 256, 0));
+        if (fused) EDK_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n[4], kf, 256, fs));
+        per_sm = std::min({n[0], n[1], fused ? n[4] : n[2], n[2], n[3]});
         return EDK_OK;
       });
     });
+    EDK_RETURN_IF(s);
+    // at least 256 rows a block, at most the resident blocks
+    const int64_t want = std::max<int64_t>(1, (totalD + 255) / 256);
+    G = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)nsm * std::max(per_sm, 1), want));
+    return EDK_OK;
   }
 
   const BOp* d_ops() const { return dops.as<BOp>(); }
@@ -663,50 +968,73 @@ struct BatchEngine {
     });
   }
 
+  RowSplit rsplit() const {
+    return RowSplit{splitops.as<SplitOp>(), splitT.as<int64_t>(), nops};
+  }
+
+  void launch_split() {
+    k_bsplit<<<1, 1024, 0, st>>>(d_ops(), nops, G, ncap, done.as<int>(), splitops.as<SplitOp>(),
+                                 splitT.as<int64_t>());
+  }
+
   template <class XT>
   edk_status launch_dots(const XT* x) {
-    size_t smem = (size_t)8 * ncap * sizeof(double2);
     return with_vt(vdt, [&](auto vp) -> edk_status {
       using VV = std::remove_pointer_t<decltype(vp)>;
-      auto kern = k_bdots<VV, XT>;
-      kern<<<(unsigned)nchunks, 256, smem, st>>>(d_ops(), chunk2op.as<int>(), V.as<VV>(), x,
-                                                 part.as<double2>(), step.as<int>(), done.as<int>());
+      k_rdots<VV, XT><<<(unsigned)G, 256, 0, st>>>(d_ops(), rsplit(), V.as<VV>(), x,
+                                                   part.as<double2>(), step.as<int>(),
+                                                   done.as<int>());
       return EDK_OK;
     });
   }
 
   template <class WI, class WO>
   edk_status launch_update(const double2* coef, const WI* win, WO* wout, bool norm, int zero) {
-    size_t smem = (size_t)ncap * sizeof(double2);
+    const size_t smem = (size_t)(ncap + 8) * sizeof(double2);
     return with_vt(vdt, [&](auto vp) -> edk_status {
       using VV = std::remove_pointer_t<decltype(vp)>;
-      auto kern = k_bupdate<VV, WI, WO>;
-      kern<<<(unsigned)ntiles, 256, smem, st>>>(d_ops(), tile2op.as<int>(), ncap, V.as<VV>(),
-                                                coef, win, wout,
-                                                norm ? normpart.as<double>() : nullptr,
-                                                step.as<int>(), done.as<int>(), zero);
+      k_rupdate<VV, WI, WO><<<(unsigned)G, 256, smem, st>>>(
+          d_ops(), rsplit(), ncap, V.as<VV>(), coef, win, wout,
+          norm ? normpart.as<double>() : nullptr, step.as<int>(), done.as<int>(), zero);
+      return EDK_OK;
+    });
+  }
+
+  template <class WI, class WO>
+  edk_status launch_update_dots(const double2* coef, const WI* win, WO* wout) {
+    const size_t smem = (size_t)(9 * ncap + 8) * sizeof(double2);
+    return with_vt(vdt, [&](auto vp) -> edk_status {
+      using VV = std::remove_pointer_t<decltype(vp)>;
+      k_rupdate_dots<VV, WI, WO><<<(unsigned)G, 256, smem, st>>>(
+          d_ops(), rsplit(), ncap, V.as<VV>(), coef, win, wout, part.as<double2>(),
+          step.as<int>(), done.as<int>());
       return EDK_OK;
     });
   }
 
   // one Lanczos step for every live operator (graph-capturable)
   edk_status enqueue_step() {
+    launch_split();
     EDK_RETURN_IF(launch_apply());
     edk_status s = with_vt(vdt, [&](auto vp) -> edk_status {
       using VV = std::remove_pointer_t<decltype(vp)>;
       return with_vt(wdt, [&](auto wp) -> edk_status {
         using WD = std::remove_pointer_t<decltype(wp)>;
         EDK_RETURN_IF(launch_dots<VV>(wt.as<VV>()));
-        k_breduce<<<dim3((ncap + 7) / 8, nops), 256, 0, st>>>(d_ops(), ncap, part.as<double2>(),
+        k_breduce<<<dim3((ncap + 7) / 8, nops), 256, 0, st>>>(splitops.as<SplitOp>(), ncap, part.as<double2>(),
                                                              coef1.as<double2>(),
                                         step.as<int>(), done.as<int>());
-        EDK_RETURN_IF((launch_update<VV, WD>(coef1.as<double2>(), wt.as<VV>(), w.as<WD>(), false, 0)));
-        EDK_RETURN_IF(launch_dots<WD>(w.as<WD>()));
-        k_breduce<<<dim3((ncap + 7) / 8, nops), 256, 0, st>>>(d_ops(), ncap, part.as<double2>(),
+        if (fused) {
+          EDK_RETURN_IF((launch_update_dots<VV, WD>(coef1.as<double2>(), wt.as<VV>(), w.as<WD>())));
+        } else {
+          EDK_RETURN_IF((launch_update<VV, WD>(coef1.as<double2>(), wt.as<VV>(), w.as<WD>(), false, 0)));
+          EDK_RETURN_IF(launch_dots<WD>(w.as<WD>()));
+        }
+        k_breduce<<<dim3((ncap + 7) / 8, nops), 256, 0, st>>>(splitops.as<SplitOp>(), ncap, part.as<double2>(),
                                                              coef2.as<double2>(),
                                         step.as<int>(), done.as<int>());
         EDK_RETURN_IF((launch_update<WD, WD>(coef2.as<double2>(), w.as<WD>(), w.as<WD>(), true, 0)));
-        k_bfinish<<<nops, 256, 0, st>>>(d_ops(), ncap, m, normpart.as<double>(),
+        k_bfinish<<<nops, 256, 0, st>>>(splitops.as<SplitOp>(), ncap, m, normpart.as<double>(),
                                         coef1.as<double2>(), alpha.as<double>(), beta.as<double>(),
                                         invb.as<double>(), nsteps.as<int>(), step.as<int>(),
                                         done.as<int>(), 0);
@@ -727,13 +1055,14 @@ struct BatchEngine {
   edk_status setup(const void* start_dev) {
     int minus1 = -1;
     EDK_TRY_CUDA(cudaMemcpyAsync(step.p, &minus1, sizeof(int), cudaMemcpyHostToDevice, st));
+    launch_split();
     edk_status s = with_vt(vdt, [&](auto vp) -> edk_status {
       using VV = std::remove_pointer_t<decltype(vp)>;
       return with_vt(wdt, [&](auto wp) -> edk_status {
         using WD = std::remove_pointer_t<decltype(wp)>;
         EDK_RETURN_IF((launch_update<WD, WD>(coef1.as<double2>(), (const WD*)start_dev,
                                              w.as<WD>(), true, 1)));
-        k_bfinish<<<nops, 256, 0, st>>>(d_ops(), ncap, m, normpart.as<double>(),
+        k_bfinish<<<nops, 256, 0, st>>>(splitops.as<SplitOp>(), ncap, m, normpart.as<double>(),
                                         coef1.as<double2>(), alpha.as<double>(), beta.as<double>(),
                                         invb.as<double>(), nsteps.as<int>(), step.as<int>(),
                                         done.as<int>(), 1);
