@@ -241,13 +241,15 @@ __device__ __forceinline__ int split_owner(int64_t r, int64_t T, int G) {
   return (int)b;
 }
 
-// One block of 1024 threads: the running operators' row offsets, blocks and
-// partial-sum slots for this step.
+// One block of 1024 threads, first in every step: advances the step counter
+// and sets the running operators' row offsets, blocks and partial-sum slots.
 // The grid's first G' = min(G, ceil(T / 128)) blocks share the rows, so each
 // has at least one and every slot of an operator is written.
 __global__ void __launch_bounds__(1024) k_bsplit(const BOp* __restrict__ ops, int nops, int Gmax,
                                                  int ncap, const int* __restrict__ done,
-                                                 SplitOp* __restrict__ sp, int64_t* __restrict__ TG) {
+                                                 SplitOp* __restrict__ sp, int64_t* __restrict__ TG,
+                                                 int* __restrict__ step, int advance) {
+  if (advance && threadIdx.x == 0) *step += 1;  // the step this launch opens
   __shared__ int64_t s_warp[32];
   const int per = (nops + 1023) / 1024;
   const int q0 = min(nops, (int)threadIdx.x * per), q1 = min(nops, q0 + per);
@@ -683,8 +685,6 @@ __global__ void __launch_bounds__(256) k_bscale(const BOp* __restrict__ ops,
   s2(V + o.voff + (int64_t)col * o.D + r, make_double2(v.x * sc, v.y * sc));
 }
 
-__global__ void k_bnext(int* step) { *step += 1; }
-
 // out_q = V_q[:, 0:nc_q] c_q (coefficients per operator, FP64 output)
 template <class VV, class OV>
 __global__ void __launch_bounds__(256) k_bcombine(const BOp* __restrict__ ops,
@@ -972,9 +972,9 @@ struct BatchEngine {
     return RowSplit{splitops.as<SplitOp>(), splitT.as<int64_t>(), nops};
   }
 
-  void launch_split() {
+  void launch_split(int advance) {
     k_bsplit<<<1, 1024, 0, st>>>(d_ops(), nops, G, ncap, done.as<int>(), splitops.as<SplitOp>(),
-                                 splitT.as<int64_t>());
+                                 splitT.as<int64_t>(), step.as<int>(), advance);
   }
 
   template <class XT>
@@ -1014,25 +1014,25 @@ struct BatchEngine {
 
   // one Lanczos step for every live operator (graph-capturable)
   edk_status enqueue_step() {
-    launch_split();
+    launch_split(1);
     EDK_RETURN_IF(launch_apply());
     edk_status s = with_vt(vdt, [&](auto vp) -> edk_status {
       using VV = std::remove_pointer_t<decltype(vp)>;
       return with_vt(wdt, [&](auto wp) -> edk_status {
         using WD = std::remove_pointer_t<decltype(wp)>;
         EDK_RETURN_IF(launch_dots<VV>(wt.as<VV>()));
-        k_breduce<<<dim3((ncap + 7) / 8, nops), 256, 0, st>>>(splitops.as<SplitOp>(), ncap, part.as<double2>(),
-                                                             coef1.as<double2>(),
-                                        step.as<int>(), done.as<int>());
+        k_breduce<<<dim3((ncap + 7) / 8, nops), 256, 0, st>>>(
+            splitops.as<SplitOp>(), ncap, part.as<double2>(), coef1.as<double2>(), step.as<int>(),
+            done.as<int>());
         if (fused) {
           EDK_RETURN_IF((launch_update_dots<VV, WD>(coef1.as<double2>(), wt.as<VV>(), w.as<WD>())));
         } else {
           EDK_RETURN_IF((launch_update<VV, WD>(coef1.as<double2>(), wt.as<VV>(), w.as<WD>(), false, 0)));
           EDK_RETURN_IF(launch_dots<WD>(w.as<WD>()));
         }
-        k_breduce<<<dim3((ncap + 7) / 8, nops), 256, 0, st>>>(splitops.as<SplitOp>(), ncap, part.as<double2>(),
-                                                             coef2.as<double2>(),
-                                        step.as<int>(), done.as<int>());
+        k_breduce<<<dim3((ncap + 7) / 8, nops), 256, 0, st>>>(
+            splitops.as<SplitOp>(), ncap, part.as<double2>(), coef2.as<double2>(), step.as<int>(),
+            done.as<int>());
         EDK_RETURN_IF((launch_update<WD, WD>(coef2.as<double2>(), w.as<WD>(), w.as<WD>(), true, 0)));
         k_bfinish<<<nops, 256, 0, st>>>(splitops.as<SplitOp>(), ncap, m, normpart.as<double>(),
                                         coef1.as<double2>(), alpha.as<double>(), beta.as<double>(),
@@ -1042,7 +1042,6 @@ struct BatchEngine {
                                                            w.as<WD>(), V.as<VV>(),
                                                            invb.as<double>(), step.as<int>(),
                                                            done.as<int>());
-        k_bnext<<<1, 1, 0, st>>>(step.as<int>());
         return EDK_OK;
       });
     });
@@ -1055,7 +1054,7 @@ struct BatchEngine {
   edk_status setup(const void* start_dev) {
     int minus1 = -1;
     EDK_TRY_CUDA(cudaMemcpyAsync(step.p, &minus1, sizeof(int), cudaMemcpyHostToDevice, st));
-    launch_split();
+    launch_split(0);
     edk_status s = with_vt(vdt, [&](auto vp) -> edk_status {
       using VV = std::remove_pointer_t<decltype(vp)>;
       return with_vt(wdt, [&](auto wp) -> edk_status {
@@ -1070,7 +1069,6 @@ struct BatchEngine {
                                                            w.as<WD>(), V.as<VV>(),
                                                            invb.as<double>(), step.as<int>(),
                                                            done.as<int>());
-        k_bnext<<<1, 1, 0, st>>>(step.as<int>());
         return EDK_OK;
       });
     });
