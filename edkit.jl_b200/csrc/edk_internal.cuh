@@ -259,11 +259,13 @@ constexpr int kPlanWindow = 256;  // rows per window of a row plan (and per thre
 // Device view of a row plan: slot k of window w describes row
 // rw[k] & kPlanRowMask of that window (rows sorted by their number of hits).
 struct RowPlanDev {
-  const uint32_t* st;     // row state (L <= 32)
-  const uint32_t* rk;     // colex rank of the row state (the row itself for complete sectors)
-  const uint32_t* rw;     // row | norm class << 27; ~0u pads the last window
-  const uint32_t* rkw;    // rank of the state with bits 0 and L-1 exchanged (the
-                          // wrap-around bond of a nearest-neighbour family), or ~0u
+  // one 16-byte slot per row, read with one load:
+  //   x = row | norm class << 27 (~0u pads the last window)
+  //   y = row state (L <= 32)
+  //   z = colex rank of the row state (the row itself for complete sectors)
+  //   w = rank of the state with bits 0 and L-1 exchanged (the wrap-around
+  //       bond of a nearest-neighbour family), or ~0u
+  const uint4* slot;
   const double* dg;       // diagonal of the row (operators with diagonal-only generic terms), or null
   const uint32_t* binom;  // binom[p * 33 + k] = C(p, k), p < 32
   int64_t nslots;         // windows * 256
@@ -272,7 +274,7 @@ constexpr uint32_t kPlanRowMask = (1u << 27) - 1u;
 
 struct OpDev {
   SellDev sell;
-  RowPlanDev plan;          // row plan of the rank-searched fast path (plan.rw null: none)
+  RowPlanDev plan;          // row plan of the rank-searched fast path (plan.slot null: none)
   int nfam;
   const FamDev* fam;
   int nterm;
@@ -326,7 +328,7 @@ struct edk_operator {
   int tps = 1;            // threads per state of the fast path (1, 2 or 4; autotuned)
   // row plan of the fast path on rank-searched sectors (edk_plan.cu): built on
   // first use; plan_state 0 not built, 1 built, -1 not available
-  edk::DevBuf p_st, p_rk, p_rw, p_rkw, p_dg, p_binom, p_bad;
+  edk::DevBuf p_slot, p_dg, p_binom, p_bad;
   int plan_state = 0;
   bool use_plan = true;   // tps == 1 on a rank-searched sector runs the plan kernel
   int use_block = -1;     // several right-hand sides through one SpMM: 1 yes, 0 no, -1 auto

@@ -27,10 +27,7 @@ template <int BK>
 __global__ void __launch_bounds__(256) k_plan_build(BasisDev b, OpDev op, FFParams ff,
                                                     int want_diag,
                                                     const uint32_t* __restrict__ binom,
-                                                    uint32_t* __restrict__ st_o,
-                                                    uint32_t* __restrict__ rk_o,
-                                                    uint32_t* __restrict__ rw_o,
-                                                    uint32_t* __restrict__ rkw_o,
+                                                    uint4* __restrict__ slot_o,
                                                     double* __restrict__ dg_o,
                                                     int* __restrict__ bad) {
   __shared__ int s_key[kPlanWindow];
@@ -79,10 +76,7 @@ __global__ void __launch_bounds__(256) k_plan_build(BasisDev b, OpDev op, FFPara
     pos += (ku < key) || (ku == key && u < t);
   }
   const int64_t slot = r0 + pos;
-  st_o[slot] = s;
-  rk_o[slot] = rk;
-  rw_o[slot] = rw;
-  rkw_o[slot] = rkw;
+  slot_o[slot] = make_uint4(rw, s, rk, rkw);
   if (want_diag) dg_o[slot] = dr;
 }
 
@@ -160,10 +154,7 @@ edk_status build_plan_kind(edk_operator* op, const FFParams& ff, int want_diag) 
   const int64_t nwin = (b.D + kPlanWindow - 1) / kPlanWindow;
   const int64_t ns = nwin * kPlanWindow;
   cudaStream_t st = op->stream;
-  EDK_RETURN_IF(op->p_st.alloc(ns * 4));
-  EDK_RETURN_IF(op->p_rk.alloc(ns * 4));
-  EDK_RETURN_IF(op->p_rw.alloc(ns * 4));
-  EDK_RETURN_IF(op->p_rkw.alloc(ns * 4));
+  EDK_RETURN_IF(op->p_slot.alloc(ns * sizeof(uint4)));
   if (want_diag) EDK_RETURN_IF(op->p_dg.alloc(ns * 8));
   EDK_RETURN_IF(op->p_bad.alloc(sizeof(int)));
   std::vector<uint32_t> binom(32 * 33, 0);
@@ -177,8 +168,7 @@ edk_status build_plan_kind(edk_operator* op, const FFParams& ff, int want_diag) 
                                cudaMemcpyHostToDevice, st));
   EDK_TRY_CUDA(cudaMemsetAsync(op->p_bad.p, 0, sizeof(int), st));
   k_plan_build<BK><<<(unsigned)nwin, kPlanWindow, 0, st>>>(
-      b, op->dev, ff, want_diag, op->p_binom.as<uint32_t>(), op->p_st.as<uint32_t>(),
-      op->p_rk.as<uint32_t>(), op->p_rw.as<uint32_t>(), op->p_rkw.as<uint32_t>(),
+      b, op->dev, ff, want_diag, op->p_binom.as<uint32_t>(), op->p_slot.as<uint4>(),
       want_diag ? op->p_dg.as<double>() : nullptr, op->p_bad.as<int>());
   EDK_TRY_CUDA(cudaGetLastError());
   int bad = 0;
@@ -193,10 +183,7 @@ edk_status build_plan_kind(edk_operator* op, const FFParams& ff, int want_diag) 
 }
 
 void plan_release(edk_operator* op) {
-  op->p_st.release();
-  op->p_rk.release();
-  op->p_rw.release();
-  op->p_rkw.release();
+  op->p_slot.release();
   op->p_dg.release();
   op->p_binom.release();
   op->dev.plan = RowPlanDev{};
@@ -238,10 +225,7 @@ edk_status plan_ensure(edk_operator* op) {
     return rc;
   }
   RowPlanDev& pl = op->dev.plan;
-  pl.st = op->p_st.as<uint32_t>();
-  pl.rk = op->p_rk.as<uint32_t>();
-  pl.rw = op->p_rw.as<uint32_t>();
-  pl.rkw = op->p_rkw.as<uint32_t>();
+  pl.slot = op->p_slot.as<uint4>();
   pl.dg = want_diag ? op->p_dg.as<double>() : nullptr;
   pl.binom = op->p_binom.as<uint32_t>();
   pl.nslots = ((b.D + kPlanWindow - 1) / kPlanWindow) * kPlanWindow;

@@ -16,9 +16,9 @@
 // What the plan removes from every product: the per-block sort of the rows by
 // hit count (done once when the plan is built: rows are ordered inside each
 // 256-row window, so the 32 lanes of a warp walk equally long hit lists), the
-// per-row reads of the 8-byte state and the 8-byte norm (a 4-byte state, rank
-// and row word per slot instead), and the walk over the set bits for the
-// wrap-around bond (its target rank is kept per slot).
+// per-row reads of the 8-byte state and the 8-byte norm (one 16-byte slot of
+// state, rank, row word and wrap-around rank instead), and the walk over the
+// set bits for the wrap-around bond.
 #pragma once
 
 #include <type_traits>
@@ -52,11 +52,10 @@ __device__ __forceinline__ void plan_row(const BasisDev& b, const OpDev& op, con
                                          int accumulate) {
   using A = typename VTraits<VT>::A;
   const RowPlanDev& pl = op.plan;
-  const uint32_t rw = __ldg(pl.rw + slot);
+  const uint4 e = __ldg(pl.slot + slot);
+  const uint32_t rw = e.x;
   if (rw == ~0u) return;
-  const uint32_t st = __ldg(pl.st + slot);
-  const uint32_t rs = __ldg(pl.rk + slot);
-  const uint32_t rkw = __ldg(pl.rkw + slot);
+  const uint32_t st = e.y, rs = e.z, rkw = e.w;
   const int64_t i = (int64_t)(rw & kPlanRowMask);
   // 1 / R of the row, rounded as the tile form rounds it (coef[c].x = R_c)
   const A invRi = BK == BK_PROJ_RANK ? (A)1 : (A)(1.0 / t.coef[rw >> 27].x);
