@@ -529,13 +529,14 @@ __global__ void __launch_bounds__(256, kSplitBlocks) k_rupdate(const BOp* __rest
 }
 
 // The first sweep's update and the second sweep's dot products in one pass,
-// 256 rows (one per thread) at a time: wout_q = win_q - V_q[:, 0:ncols]
-// coef_q, then, with the result still in registers, its dot products with
-// the same rows of every column, added per warp into shared memory; at the
-// end of the piece the warps' sums go to part[pofs_q + c * nslot_q + slot].
-// The dot products walk the columns in reverse, so the ones the update read
-// last, the most likely to be still in L2, are read again first.
-// Shared memory: ncap + 8 coefficients and 8 x ncap per-warp sums (double2).
+// 256 rows at a time.  Update: one thread per row, wout = win - V coef over
+// all columns; the result (as stored) goes to shared memory.  Dot products:
+// one warp per column (warps take every eighth column, newest first, so the
+// columns the update read last, the most likely to be still in L2, are read
+// again first), each lane over eight of the 256 rows, one warp reduction per
+// column; the sums build up per column in shared memory and go to
+// part[pofs_q + c * nslot_q + slot] at the end of the piece.
+// Shared memory: ncap + 8 coefficients and ncap column sums (double2).
 template <class VV, class WI, class WO>
 __global__ void __launch_bounds__(256, kSplitBlocks) k_rupdate_dots(const BOp* __restrict__ ops, RowSplit rs,
                                                       int ncap, const VV* __restrict__ V,
@@ -548,6 +549,7 @@ __global__ void __launch_bounds__(256, kSplitBlocks) k_rupdate_dots(const BOp* _
   extern __shared__ double2 s_dyn[];
   double2* s_coef = s_dyn;
   double2* s_acc = s_dyn + ncap + 8;
+  __shared__ double2 s_w[256];
   constexpr bool CX = IsCx<VV>::v || IsCx<WI>::v || IsCx<WO>::v;
   constexpr int U = CX ? 4 : 8;
   const int ncols = *step + 1;
@@ -555,19 +557,19 @@ __global__ void __launch_bounds__(256, kSplitBlocks) k_rupdate_dots(const BOp* _
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for_block_rows(ops, rs, [&](int q, const BOp& o, int64_t r0, int64_t r1, int slot, const SplitOp& sq) {
     if (done[q]) return;
-    __syncthreads();  // the previous piece's shared sums are written out
+    __syncthreads();  // the previous piece's column sums are written out
     for (int c = threadIdx.x; c < npad; c += blockDim.x)
       s_coef[c] = c < ncols ? coef[(int64_t)q * ncap + c] : make_double2(0.0, 0.0);
-    for (int i = threadIdx.x; i < 8 * ncols; i += blockDim.x)
-      s_acc[(i / ncols) * ncap + i % ncols] = make_double2(0.0, 0.0);
+    for (int c = threadIdx.x; c < ncols; c += blockDim.x) s_acc[c] = make_double2(0.0, 0.0);
     __syncthreads();
     const int64_t D = o.D;
     const VV* Vq = V + o.voff;
     for (int64_t rb = r0; rb < r1; rb += 256) {
       const int64_t r = rb + threadIdx.x;
-      const bool on = r < r1;
-      double2 acc[1] = {on ? l2(win + o.woff + r) : make_double2(0.0, 0.0)};
-      if (on) {
+      const int nrow = (int)min((int64_t)256, r1 - rb);
+      double2 acc[1] = {make_double2(0.0, 0.0)};
+      if (r < r1) {
+        acc[0] = l2(win + o.woff + r);
         for (int c = 0; c < npad; c += U) {
           const VV* Vc[U];
 #pragma unroll
@@ -579,45 +581,46 @@ __global__ void __launch_bounds__(256, kSplitBlocks) k_rupdate_dots(const BOp* _
         wout[o.woff + r] = t;
         acc[0] = l2(&t);  // the dot products see the stored value
       }
-      for (int c = npad - U; c >= 0; c -= U) {
-        const VV* Vc[U];
+      s_w[threadIdx.x] = acc[0];
+      __syncthreads();
+      // two columns (c and c - 8) per pass: sixteen loads in flight a lane
+      for (int c = ncols - 1 - warp; c >= 0; c -= 16) {
+        const int c2 = c >= 8 ? c - 8 : c;
+        const VV* Va = Vq + (int64_t)c * D + rb;
+        const VV* Vb = Vq + (int64_t)c2 * D + rb;
+        double ar = 0.0, ai = 0.0, br = 0.0, bi = 0.0;
 #pragma unroll
-        for (int u = 0; u < U; ++u) Vc[u] = Vq + (int64_t)min(c + u, ncols - 1) * D + r;
-        double a[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) a[u] = 0.0;
-        if (on) {
-          double2 v[U];
-#pragma unroll
-          for (int u = 0; u < U; ++u) v[u] = l2(Vc[u]);
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            if constexpr (CX) {
-              a[2 * u] = v[u].x * acc[0].x + v[u].y * acc[0].y;
-              a[2 * u + 1] = v[u].x * acc[0].y - v[u].y * acc[0].x;
-            } else {
-              a[u] = v[u].x * acc[0].x;
+        for (int k = 0; k < 8; ++k) {
+          const int i = lane + 32 * k;
+          if (i < nrow) {
+            const double2 va = l2(Va + i), vb = l2(Vb + i), x = s_w[i];
+            ar += va.x * x.x + va.y * x.y;
+            br += vb.x * x.x + vb.y * x.y;
+            if (CX) {
+              ai += va.x * x.y - va.y * x.x;
+              bi += vb.x * x.y - vb.y * x.x;
             }
           }
         }
-        const double t = wsum8(a, lane);
-        if ((lane & 3) == 0) {
-          const int vi = lane >> 2;
-          const int col = CX ? c + (vi >> 1) : c + vi;
-          if (col < ncols) reinterpret_cast<double*>(s_acc + warp * ncap + col)[CX ? (vi & 1) : 0] += t;
+        ar = wsum(ar);
+        br = wsum(br);
+        if (CX) {
+          ai = wsum(ai);
+          bi = wsum(bi);
+        }
+        if (lane == 0) {
+          s_acc[c].x += ar;
+          s_acc[c].y += ai;
+          if (c2 != c) {
+            s_acc[c2].x += br;
+            s_acc[c2].y += bi;
+          }
         }
       }
+      __syncthreads();  // s_w is rewritten by the next rows
     }
-    __syncthreads();
-    for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
-      double sr = 0.0, si = 0.0;
-#pragma unroll
-      for (int ww = 0; ww < 8; ++ww) {
-        sr += s_acc[ww * ncap + c].x;
-        si += s_acc[ww * ncap + c].y;
-      }
-      part[sq.pofs + (int64_t)c * sq.nslot + slot] = make_double2(sr, si);
-    }
+    for (int c = threadIdx.x; c < ncols; c += blockDim.x)
+      part[sq.pofs + (int64_t)c * sq.nslot + slot] = s_acc[c];
   });
 }
 
@@ -853,7 +856,7 @@ struct BatchEngine {
       set_error("batch Lanczos: too many steps for the shared-memory coefficients (max 12800)");
       return EDK_UNSUPPORTED;
     }
-    const size_t fs = us + (size_t)8 * ncap * sizeof(double2);  // + per-warp sums
+    const size_t fs = us + (size_t)ncap * sizeof(double2);  // + column sums
     fused = fs <= 200 * 1024;
     int dev = 0, nsm = 0;
     EDK_TRY_CUDA(cudaGetDevice(&dev));
@@ -1002,7 +1005,7 @@ struct BatchEngine {
 
   template <class WI, class WO>
   edk_status launch_update_dots(const double2* coef, const WI* win, WO* wout) {
-    const size_t smem = (size_t)(9 * ncap + 8) * sizeof(double2);
+    const size_t smem = (size_t)(2 * ncap + 8) * sizeof(double2);
     return with_vt(vdt, [&](auto vp) -> edk_status {
       using VV = std::remove_pointer_t<decltype(vp)>;
       k_rupdate_dots<VV, WI, WO><<<(unsigned)G, 256, smem, st>>>(
