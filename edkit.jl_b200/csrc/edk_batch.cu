@@ -423,12 +423,26 @@ __global__ void __launch_bounds__(256) k_breduce(const SplitOp* __restrict__ sp,
   const int lane = threadIdx.x & 31;
   const SplitOp& o = sp[q];
   const double2* pc = part + o.pofs + (int64_t)c * o.nslot;
-  double sr = 0.0, si = 0.0;
-  for (int k = lane; k < o.nslot; k += 32) {
-    const double2 v = pc[k];
-    sr += v.x;
-    si += v.y;
+  // four independent loads in flight a lane (a large operator has hundreds
+  // of slots and only j + 1 columns, so few warps carry the whole reduction)
+  double2 a[4] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0),
+                  make_double2(0.0, 0.0)};
+  int k = lane;
+  for (; k + 96 < o.nslot; k += 128) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double2 v = pc[k + 32 * u];
+      a[u].x += v.x;
+      a[u].y += v.y;
+    }
   }
+  for (; k < o.nslot; k += 32) {
+    const double2 v = pc[k];
+    a[0].x += v.x;
+    a[0].y += v.y;
+  }
+  double sr = (a[0].x + a[1].x) + (a[2].x + a[3].x);
+  double si = (a[0].y + a[1].y) + (a[2].y + a[3].y);
   sr = wsum(sr);
   si = wsum(si);
   if (lane == 0) coef[(int64_t)q * ncap + c] = make_double2(sr, si);

@@ -138,3 +138,21 @@ def test_mixed_ensemble_all_four_levels(ek, O):
         assert np.allclose(emx[q], e64[q], rtol=0, atol=1e-9 * abs(e64[q][0])), q
         if dense[q] is not None:
             assert np.allclose(e64[q], dense[q], rtol=0, atol=1e-9 * abs(dense[q][0])), q
+
+
+def test_large_krylov_capacity_takes_the_two_pass_sweep(ek, O):
+    """With room for 7,000 Krylov vectors the fused update + dot-product pass
+    no longer fits its shared memory, and the second sweep runs as separate
+    dot-product and update passes: same eigenvalues as the fused path and the
+    dense spectrum."""
+    ops, dense = [], []
+    for L, k in ((14, 0), (16, 3), (14, 5)):
+        b = ek.TranslationalBasis(L=L, N=L // 2, k=k)
+        ops.append(ek.trans_inv_operator(xxz(ek.spin, 1.5), 2, b))
+        Ho = O.trans_inv_operator(xxz(O.spin, 1.5), 2, O.translational(L, k=k, N=L // 2))
+        dense.append(np.linalg.eigvalsh(Ho.dense())[:2])
+    big, _ = ek.batch_lanczos_e0(ops, m=7000, nev=2, tol=1e-12, check_every=5)
+    small, _ = ek.batch_lanczos_e0(ops, m=150, nev=2, tol=1e-12, check_every=5)
+    for q in range(3):
+        assert np.allclose(big[q], dense[q], rtol=0, atol=1e-10 * abs(dense[q][0])), q
+        assert np.allclose(big[q], small[q], rtol=0, atol=1e-11 * abs(dense[q][0])), q
