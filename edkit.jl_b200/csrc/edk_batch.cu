@@ -206,9 +206,10 @@ struct RowSplit {
   int nops;
 };
 
-// exclusive prefix sum over a block of 1024 threads; *total gets the sum
-__device__ int64_t block_scan1024(int64_t v, int64_t* s_warp, int64_t* total) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// exclusive prefix sum over the block (blockDim.x a multiple of 32, at most
+// 1024); *total gets the sum
+__device__ int64_t block_scan(int64_t v, int64_t* s_warp, int64_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   int64_t x = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -218,17 +219,17 @@ __device__ int64_t block_scan1024(int64_t v, int64_t* s_warp, int64_t* total) {
   if (lane == 31) s_warp[warp] = x;
   __syncthreads();
   if (warp == 0) {
-    int64_t t = s_warp[lane];
+    int64_t t = lane < nw ? s_warp[lane] : 0;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int64_t y = __shfl_up_sync(0xffffffffu, t, o);
       if (lane >= o) t += y;
     }
-    s_warp[lane] = t;  // inclusive over warps
+    if (lane < nw) s_warp[lane] = t;  // inclusive over warps
   }
   __syncthreads();
   const int64_t before = (warp > 0 ? s_warp[warp - 1] : 0) + x - v;
-  *total = s_warp[31];
+  *total = s_warp[nw - 1];
   __syncthreads();
   return before;
 }
@@ -241,26 +242,25 @@ __device__ __forceinline__ int split_owner(int64_t r, int64_t T, int G) {
   return (int)b;
 }
 
-// One block of 1024 threads, first in every step: advances the step counter
-// and sets the running operators' row offsets, blocks and partial-sum slots.
-// The grid's first G' = min(G, ceil(T / 128)) blocks share the rows, so each
-// has at least one and every slot of an operator is written.
-__global__ void __launch_bounds__(1024) k_bsplit(const BOp* __restrict__ ops, int nops, int Gmax,
-                                                 int ncap, const int* __restrict__ done,
-                                                 SplitOp* __restrict__ sp, int64_t* __restrict__ TG,
-                                                 int* __restrict__ step, int advance) {
-  if (advance && threadIdx.x == 0) *step += 1;  // the step this launch opens
+// The running operators' row offsets, blocks and partial-sum slots, by one
+// whole block.  The grid's first G' = min(G, ceil(T / 128)) blocks share the
+// rows, so each has at least one and every slot of an operator is written.
+// The stop flags are read past L1: in k_bfinish other blocks have just set
+// them.
+__device__ void split_rows_dev(const BOp* __restrict__ ops, int nops, int Gmax, int ncap,
+                               const int* done, SplitOp* __restrict__ sp,
+                               int64_t* __restrict__ TG) {
   __shared__ int64_t s_warp[32];
-  const int per = (nops + 1023) / 1024;
+  const int per = (nops + (int)blockDim.x - 1) / (int)blockDim.x;
   const int q0 = min(nops, (int)threadIdx.x * per), q1 = min(nops, q0 + per);
   int64_t loc = 0;
-  for (int q = q0; q < q1; ++q) loc += done[q] ? 0 : ops[q].D;
+  for (int q = q0; q < q1; ++q) loc += __ldcg(done + q) ? 0 : ops[q].D;
   int64_t T = 0;
-  int64_t off = block_scan1024(loc, s_warp, &T);
+  int64_t off = block_scan(loc, s_warp, &T);
   const int G = (int)max((int64_t)1, min((int64_t)Gmax, (T + 127) / 128));
   int64_t nsl = 0;
   for (int q = q0; q < q1; ++q) {
-    const int64_t d = done[q] ? 0 : ops[q].D;
+    const int64_t d = __ldcg(done + q) ? 0 : ops[q].D;
     SplitOp o;
     o.off = off;
     o.pofs = 0;
@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(1024) k_bsplit(const BOp* __restrict__ ops, in
     off += d;
   }
   int64_t nslot_all = 0;
-  int64_t s0 = block_scan1024(nsl, s_warp, &nslot_all);
+  int64_t s0 = block_scan(nsl, s_warp, &nslot_all);
   for (int q = q0; q < q1; ++q) {
     sp[q].slot0 = s0;
     sp[q].pofs = s0 * ncap;
@@ -287,6 +287,14 @@ __global__ void __launch_bounds__(1024) k_bsplit(const BOp* __restrict__ ops, in
     TG[0] = T;
     TG[1] = G;
   }
+}
+
+// the split before the first step (one block of 1024 threads); later steps
+// get theirs from the last block of k_bfinish
+__global__ void __launch_bounds__(1024) k_bsplit(const BOp* __restrict__ ops, int nops, int Gmax,
+                                                 int ncap, const int* __restrict__ done,
+                                                 SplitOp* __restrict__ sp, int64_t* __restrict__ TG) {
+  split_rows_dev(ops, nops, Gmax, ncap, done, sp, TG);
 }
 
 template <class F>
@@ -638,51 +646,73 @@ __global__ void __launch_bounds__(256, kSplitBlocks) k_rupdate_dots(const BOp* _
   });
 }
 
-// per operator: alpha_j, beta_j, breakdown, 1/beta (one block per operator)
-__global__ void __launch_bounds__(256) k_bfinish(const SplitOp* __restrict__ sp, int ncap, int m,
+// per operator: alpha_j, beta_j, breakdown, 1/beta (one block per operator).
+// The last block to finish then closes the step: it splits the rows of the
+// operators still running for the next step's reorthogonalisation kernels
+// and advances the step counter (every block has read it by then).
+__global__ void __launch_bounds__(256) k_bfinish(const BOp* __restrict__ ops, int nops, int Gmax,
+                                                 SplitOp* __restrict__ sp,
+                                                 int64_t* __restrict__ TG,
+                                                 unsigned* __restrict__ nfinished, int ncap, int m,
                                                  const double* __restrict__ normpart,
                                                  const double2* __restrict__ coef1,
                                                  double* __restrict__ alpha,
                                                  double* __restrict__ beta,
                                                  double* __restrict__ invb,
                                                  int* __restrict__ nsteps,
-                                                 const int* __restrict__ step,
+                                                 int* __restrict__ step,
                                                  int* __restrict__ done, int setup) {
   const int q = blockIdx.x;
-  if (done[q]) return;
-  const SplitOp& o = sp[q];
-  double s = 0.0;
-  for (int k = threadIdx.x; k < o.nslot; k += blockDim.x) s += normpart[o.slot0 + k];
-  __shared__ double sh[8];
-  s = wsum(s);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x != 0) return;
-  double n2 = 0.0;
-  for (int k = 0; k < 8; ++k) n2 += sh[k];
-  const double nrm = sqrt(n2);
-  if (setup) {  // starting vector: zero or non-finite norm is an error for this operator
-    if (!isfinite(nrm)) { done[q] = 4; invb[q] = 0.0; }
-    else if (!(nrm > 0.0)) { done[q] = 3; invb[q] = 0.0; }
-    else invb[q] = 1.0 / nrm;
-    return;
-  }
   const int j = *step;
-  const double a = coef1[(int64_t)q * ncap + j].x;
-  alpha[(int64_t)q * m + j] = a;
-  beta[(int64_t)q * m + j] = nrm;
-  nsteps[q] = j + 1;
-  const double seps = 1.4901161193847656e-08;  // sqrt(eps(Float64))
-  if (nrm <= seps * fmax(1.0, fabs(a))) {
-    beta[(int64_t)q * m + j] = 0.0;
-    done[q] = 2;
-    invb[q] = 0.0;
-  } else {
-    invb[q] = 1.0 / nrm;
+  __shared__ double sh[8];
+  __shared__ bool s_last;
+  if (!done[q]) {
+    const SplitOp o = sp[q];
+    double s = 0.0;
+    for (int k = threadIdx.x; k < o.nslot; k += blockDim.x) s += normpart[o.slot0 + k];
+    s = wsum(s);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double n2 = 0.0;
+      for (int k = 0; k < 8; ++k) n2 += sh[k];
+      const double nrm = sqrt(n2);
+      if (setup) {  // starting vector: zero or non-finite norm is an error for this operator
+        if (!isfinite(nrm)) { done[q] = 4; invb[q] = 0.0; }
+        else if (!(nrm > 0.0)) { done[q] = 3; invb[q] = 0.0; }
+        else invb[q] = 1.0 / nrm;
+      } else {
+        const double a = coef1[(int64_t)q * ncap + j].x;
+        alpha[(int64_t)q * m + j] = a;
+        beta[(int64_t)q * m + j] = nrm;
+        nsteps[q] = j + 1;
+        const double seps = 1.4901161193847656e-08;  // sqrt(eps(Float64))
+        if (nrm <= seps * fmax(1.0, fabs(a))) {
+          beta[(int64_t)q * m + j] = 0.0;
+          done[q] = 2;
+          invb[q] = 0.0;
+        } else {
+          invb[q] = 1.0 / nrm;
+        }
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();  // this block's stop flag before its count
+    s_last = atomicAdd(nfinished, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  split_rows_dev(ops, nops, Gmax, ncap, done, sp, TG);
+  if (threadIdx.x == 0) {
+    *nfinished = 0;
+    *step = j + 1;
   }
 }
 
-// V_q[:, j+1] = w_q / beta (skipped past the last column)
+// V_q[:, j+1] = w_q / beta (skipped past the last column); k_bfinish has
+// advanced the step counter to j + 1
 template <class WV, class VV>
 __global__ void __launch_bounds__(256) k_bscale(const BOp* __restrict__ ops,
                                                 const int* __restrict__ tile2op, int ncap,
@@ -693,7 +723,7 @@ __global__ void __launch_bounds__(256) k_bscale(const BOp* __restrict__ ops,
   const int q = tile2op[blockIdx.x];
   if (done[q]) return;
   const BOp& o = ops[q];
-  const int col = *step + 1;
+  const int col = *step;
   if (col >= ncap) return;
   const int64_t r = (blockIdx.x - o.tile0) * (int64_t)kTile + threadIdx.x;
   if (r >= o.D) return;
@@ -759,7 +789,7 @@ struct BatchEngine {
   int64_t ntiles = 0, totalD = 0;
   int G = 1;             // blocks of the reorthogonalisation grid
   bool fused = false;    // first update and second dot products in one kernel
-  DevBuf dops, tile2op, sblk2op, splitops, splitT, V, w, wt, part, coef1, coef2, normpart, alpha, beta, invb,
+  DevBuf dops, tile2op, sblk2op, splitops, splitT, nfin, V, w, wt, part, coef1, coef2, normpart, alpha, beta, invb,
       done, step, nsteps, cbuf, cnc;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -844,6 +874,8 @@ struct BatchEngine {
     EDK_RETURN_IF(part.alloc_async((size_t)(G + nops) * ncap * sizeof(double2), st));
     EDK_RETURN_IF(splitops.alloc_async((size_t)nops * sizeof(SplitOp), st));
     EDK_RETURN_IF(splitT.alloc_async(2 * sizeof(int64_t), st));
+    EDK_RETURN_IF(nfin.alloc_async(sizeof(unsigned), st));
+    EDK_TRY_CUDA(cudaMemsetAsync(nfin.p, 0, sizeof(unsigned), st));
     EDK_RETURN_IF(coef1.alloc_async((size_t)nops * ncap * sizeof(double2), st));
     EDK_RETURN_IF(coef2.alloc_async((size_t)nops * ncap * sizeof(double2), st));
     EDK_RETURN_IF(normpart.alloc_async((size_t)(G + nops) * sizeof(double), st));
@@ -989,9 +1021,19 @@ struct BatchEngine {
     return RowSplit{splitops.as<SplitOp>(), splitT.as<int64_t>(), nops};
   }
 
-  void launch_split(int advance) {
+  void launch_split() {
     k_bsplit<<<1, 1024, 0, st>>>(d_ops(), nops, G, ncap, done.as<int>(), splitops.as<SplitOp>(),
-                                 splitT.as<int64_t>(), step.as<int>(), advance);
+                                 splitT.as<int64_t>());
+  }
+
+  // alpha / beta / stop flags, then (last block) the next step's split and
+  // the step counter
+  void launch_finish(int setup) {
+    k_bfinish<<<nops, 256, 0, st>>>(d_ops(), nops, G, splitops.as<SplitOp>(),
+                                    splitT.as<int64_t>(), nfin.as<unsigned>(), ncap, m,
+                                    normpart.as<double>(), coef1.as<double2>(),
+                                    alpha.as<double>(), beta.as<double>(), invb.as<double>(),
+                                    nsteps.as<int>(), step.as<int>(), done.as<int>(), setup);
   }
 
   template <class XT>
@@ -1031,7 +1073,6 @@ struct BatchEngine {
 
   // one Lanczos step for every live operator (graph-capturable)
   edk_status enqueue_step() {
-    launch_split(1);
     EDK_RETURN_IF(launch_apply());
     edk_status s = with_vt(vdt, [&](auto vp) -> edk_status {
       using VV = std::remove_pointer_t<decltype(vp)>;
@@ -1051,10 +1092,7 @@ struct BatchEngine {
             splitops.as<SplitOp>(), ncap, part.as<double2>(), coef2.as<double2>(), step.as<int>(),
             done.as<int>());
         EDK_RETURN_IF((launch_update<WD, WD>(coef2.as<double2>(), w.as<WD>(), w.as<WD>(), true, 0)));
-        k_bfinish<<<nops, 256, 0, st>>>(splitops.as<SplitOp>(), ncap, m, normpart.as<double>(),
-                                        coef1.as<double2>(), alpha.as<double>(), beta.as<double>(),
-                                        invb.as<double>(), nsteps.as<int>(), step.as<int>(),
-                                        done.as<int>(), 0);
+        launch_finish(0);
         k_bscale<WD, VV><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), tile2op.as<int>(), ncap,
                                                            w.as<WD>(), V.as<VV>(),
                                                            invb.as<double>(), step.as<int>(),
@@ -1071,17 +1109,14 @@ struct BatchEngine {
   edk_status setup(const void* start_dev) {
     int minus1 = -1;
     EDK_TRY_CUDA(cudaMemcpyAsync(step.p, &minus1, sizeof(int), cudaMemcpyHostToDevice, st));
-    launch_split(0);
+    launch_split();
     edk_status s = with_vt(vdt, [&](auto vp) -> edk_status {
       using VV = std::remove_pointer_t<decltype(vp)>;
       return with_vt(wdt, [&](auto wp) -> edk_status {
         using WD = std::remove_pointer_t<decltype(wp)>;
         EDK_RETURN_IF((launch_update<WD, WD>(coef1.as<double2>(), (const WD*)start_dev,
                                              w.as<WD>(), true, 1)));
-        k_bfinish<<<nops, 256, 0, st>>>(splitops.as<SplitOp>(), ncap, m, normpart.as<double>(),
-                                        coef1.as<double2>(), alpha.as<double>(), beta.as<double>(),
-                                        invb.as<double>(), nsteps.as<int>(), step.as<int>(),
-                                        done.as<int>(), 1);
+        launch_finish(1);
         k_bscale<WD, VV><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), tile2op.as<int>(), ncap,
                                                            w.as<WD>(), V.as<VV>(),
                                                            invb.as<double>(), step.as<int>(),
