@@ -899,7 +899,7 @@ struct BatchEngine {
   edk_status split_rows() {
     const size_t us = (size_t)(ncap + 8) * sizeof(double2);
     if (us > 200 * 1024) {
-      set_error("batch Lanczos: too many steps for the shared-memory coefficients (max 12800)");
+      set_error("batch Lanczos: too many steps for the shared-memory coefficients (max 12791)");
       return EDK_UNSUPPORTED;
     }
     const size_t fs = us + (size_t)ncap * sizeof(double2);  // + column sums

@@ -292,7 +292,8 @@ typedef enum {
 } edk_precision;
 
 typedef struct {
-  int32_t max_steps;     /* Lanczos steps (m) */
+  int32_t max_steps;     /* Lanczos steps (m); at most 12,791 on the batched
+                            engine (its step coefficients sit in shared memory) */
   int32_t nev;           /* number of lowest eigenvalues wanted */
   double tol;            /* relative stop tolerance on the Ritz values; 0 = run max_steps */
   int32_t check_every;   /* steps between convergence checks */
