@@ -665,44 +665,50 @@ static edk_status block_lanczos(int nops, edk_operator* const* ops,
   int steps = 0;
   bool converged = false;
 
-  auto extract = [&](int nsteps) {
+  // eigenvalues of every operator's block tridiagonal T: the blocks are put
+  // together on the host (threads over the operators), the eigenvalue step
+  // itself runs on the device (band_lowest_device)
+  std::vector<std::vector<cplx>> Aall(nops);
+  auto extract = [&](int nsteps) -> edk_status {
     const double te = wall_s();
     const int nth = (int)std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), 64));
     std::vector<std::thread> pool;
-    std::vector<std::vector<double>> res(nops);
+    std::vector<int> mqs(nops);
+    std::vector<std::vector<const double*>> Ap(nops), Bp(nops);
     auto work = [&](int t) {
       for (int q = t; q < nops; q += nth) {
         const int mq = broke_at[q] >= 0 ? broke_at[q] : nsteps;
-        std::vector<std::vector<cplx>> Aq(mq);
-        std::vector<const double*> Ap(mq), Bp(mq, nullptr);
+        mqs[q] = mq;
+        Aall[q].assign((size_t)mq * pp, cplx(0.0, 0.0));
+        Ap[q].assign(mq, nullptr);
+        Bp[q].assign(mq, nullptr);
         for (int j = 0; j < mq; ++j) {
-          Aq[j].resize(pp);
+          cplx* Aj = Aall[q].data() + (size_t)j * pp;
           const cplx* a1 = hA.data() + ((size_t)j * nops + q) * pp;
           const cplx* a2 = hA2.data() + ((size_t)j * nops + q) * pp;
           // device holds (V^H W)^T column-major = A row-major; make A
           // column-major and Hermitian
           for (int r = 0; r < p; ++r)
-            for (int c = 0; c < p; ++c) {
-              const cplx v = a1[c + (size_t)r * p] + a2[c + (size_t)r * p];
-              Aq[j][r + (size_t)c * p] = v;
-            }
+            for (int c = 0; c < p; ++c) Aj[r + (size_t)c * p] = a1[c + (size_t)r * p] + a2[c + (size_t)r * p];
           for (int r = 0; r < p; ++r)
             for (int c = r; c < p; ++c) {
-              const cplx h = 0.5 * (Aq[j][r + (size_t)c * p] + std::conj(Aq[j][c + (size_t)r * p]));
-              Aq[j][r + (size_t)c * p] = h;
-              Aq[j][c + (size_t)r * p] = std::conj(h);
+              const cplx h = 0.5 * (Aj[r + (size_t)c * p] + std::conj(Aj[c + (size_t)r * p]));
+              Aj[r + (size_t)c * p] = h;
+              Aj[c + (size_t)r * p] = std::conj(h);
             }
-          Ap[j] = reinterpret_cast<const double*>(Aq[j].data());
-          if (j >= 1) Bp[j] = reinterpret_cast<const double*>(hB.data() + ((size_t)j * nops + q) * pp);
+          Ap[q][j] = reinterpret_cast<const double*>(Aj);
+          if (j >= 1) Bp[q][j] = reinterpret_cast<const double*>(hB.data() + ((size_t)j * nops + q) * pp);
         }
-        band_lowest(Ap, Bp, p, mq, o.nev, res[q]);
       }
     };
     for (int t = 0; t < nth; ++t) pool.emplace_back(work, t);
     for (auto& th : pool) th.join();
+    std::vector<std::vector<double>> res;
+    EDK_RETURN_IF(band_lowest_device(p, o.nev, mqs, Ap, Bp, st, res));
     for (int q = 0; q < nops; ++q)
       for (int k = 0; k < o.nev; ++k) cur[(size_t)q * o.nev + k] = res[q][k];
     t_eig += wall_s() - te;
+    return EDK_OK;
   };
 
   for (int j = 0; j < m; ++j) {
@@ -749,7 +755,7 @@ static edk_status block_lanczos(int nops, edk_operator* const* ops,
     const bool check = (o.check_every > 0 && (j + 1) % o.check_every == 0) || j + 1 == m ||
                        all_broken;
     if (check) {
-      extract(j + 1);
+      EDK_RETURN_IF(extract(j + 1));
       if (o.tol > 0.0 && j + 1 < m) {
         bool conv = true;
         for (int q = 0; q < nops && conv; ++q)
@@ -764,7 +770,7 @@ static edk_status block_lanczos(int nops, edk_operator* const* ops,
       if (all_broken) break;
     }
   }
-  if (steps > 0 && std::isnan(cur[0])) extract(steps);
+  if (steps > 0 && std::isnan(cur[0])) EDK_RETURN_IF(extract(steps));
   std::memcpy(evals, cur.data(), cur.size() * sizeof(double));
   if (diag) {
     std::memset(diag, 0, sizeof(*diag));

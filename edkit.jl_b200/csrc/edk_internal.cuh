@@ -389,6 +389,14 @@ edk_status batch_lanczos(const std::vector<edk_operator*>& ops, const edk_lanczo
                          void* ritz_out = nullptr);
 // implemented in edk_util.cpp
 int tridiag_eigvals(int m, const double* a, const double* b, double* w);
+// The lowest `nev` distinct eigenvalues of block-tridiagonal Hermitian
+// matrices (operator q: m[q] blocks of p x p, A[q][j] on the diagonal and
+// B[q][j], j >= 1, below it, column-major interleaved complex on the host),
+// on the device (edk_band.cu); NaN where fewer are found.
+edk_status band_lowest_device(int p, int nev, const std::vector<int>& m,
+                              const std::vector<std::vector<const double*>>& A,
+                              const std::vector<std::vector<const double*>>& B,
+                              cudaStream_t st, std::vector<std::vector<double>>& out);
 int tridiag_eigen(int m, const double* a, const double* b, double* w, double* Q);
 double elapsed_ms(cudaEvent_t a, cudaEvent_t b);
 }  // namespace edk
