@@ -220,8 +220,9 @@ typedef struct {
 } edk_block_lanczos_diag;
 void edk_block_lanczos_default_opts(edk_block_lanczos_opts* opts);
 
-/* The eigenvalue step of edk_block_lanczos on a block-tridiagonal matrix the
- * caller holds (host only, no device work): A = m diagonal blocks (p x p,
+/* The eigenvalue step of edk_block_lanczos (which runs it on the device) on
+ * a block-tridiagonal matrix the caller holds, computed on the host with no
+ * device work: A = m diagonal blocks (p x p,
  * column-major complex, interleaved re/im, Hermitian), B = m-1 sub-diagonal
  * blocks T(j+1, j).  out = the lowest nev distinct eigenvalues, copies that a
  * block Lanczos run without full re-orthogonalisation creates removed by the
