@@ -4,8 +4,8 @@
 // EDKit's Krylov loop (_lanczos_build!, src/algorithms/TimeEvolution.jl:250-306)
 // advances one vector.  The block form advances p vectors per operator:
 //
-//   W = H V_j;  W -= V_j A_j + V_{j-1} C  (classical block Gram-Schmidt
-//   against the two previous blocks, twice); W = V_{j+1} B_{j+1} by
+//   W = H V_j;  W -= V_j A_j + V_{j-1} C  (one classical block Gram-Schmidt
+//   pass against the two previous blocks); W = V_{j+1} B_{j+1} by
 //   Cholesky-QR, twice.
 //
 // and the lowest eigenvalues come from the Hermitian block-tridiagonal
@@ -518,13 +518,13 @@ static edk_status block_lanczos(int nops, edk_operator* const* ops,
     }
   }
 
-  DevBuf d_ops, ring0, ring1, ring2, part, Q1, Q2, Q1b, Q2b, G, Rinv, R1, R2, Bm, flags, colx, coly;
+  DevBuf d_ops, ring0, ring1, ring2, part, Q1, Q2, G, Rinv, R1, R2, Bm, flags, colx, coly;
   EDK_RETURN_IF(d_ops.alloc(sizeof(SpmmOp) * nops));
   EDK_RETURN_IF(ring0.alloc(slot * sizeof(double2)));
   EDK_RETURN_IF(ring1.alloc(slot * sizeof(double2)));
   EDK_RETURN_IF(ring2.alloc(slot * sizeof(double2)));
   EDK_RETURN_IF(part.alloc((size_t)nops * S * pp * sizeof(double2)));
-  for (DevBuf* bf : {&Q1, &Q2, &Q1b, &Q2b, &G, &Rinv, &R1, &R2, &Bm})
+  for (DevBuf* bf : {&Q1, &Q2, &G, &Rinv, &R1, &R2, &Bm})
     EDK_RETURN_IF(bf->alloc((size_t)nops * pp * sizeof(double2)));
   EDK_RETURN_IF(flags.alloc(nops * sizeof(int)));
   if (any_generic) {
@@ -655,9 +655,9 @@ static edk_status block_lanczos(int nops, edk_operator* const* ops,
   EDK_RETURN_IF(cholqr(W, U));
   std::swap(V, W);  // V = V_1; U (zero rows not needed: j = 1 skips it)
 
-  // per step host copies: A parts (two passes) and B
+  // per step host copies: A and B
   const int m = o.max_steps;
-  std::vector<cplx> hA((size_t)m * nops * pp), hA2((size_t)m * nops * pp),
+  std::vector<cplx> hA((size_t)m * nops * pp),
       hB((size_t)(m + 1) * nops * pp);
   std::vector<int> hflag(nops, 0), broke_at(nops, -1);
   std::vector<double> cur((size_t)nops * o.nev, NAN), prev((size_t)nops * o.nev, NAN);
@@ -685,11 +685,10 @@ static edk_status block_lanczos(int nops, edk_operator* const* ops,
         for (int j = 0; j < mq; ++j) {
           cplx* Aj = Aall[q].data() + (size_t)j * pp;
           const cplx* a1 = hA.data() + ((size_t)j * nops + q) * pp;
-          const cplx* a2 = hA2.data() + ((size_t)j * nops + q) * pp;
           // device holds (V^H W)^T column-major = A row-major; make A
           // column-major and Hermitian
           for (int r = 0; r < p; ++r)
-            for (int c = 0; c < p; ++c) Aj[r + (size_t)c * p] = a1[c + (size_t)r * p] + a2[c + (size_t)r * p];
+            for (int c = 0; c < p; ++c) Aj[r + (size_t)c * p] = a1[c + (size_t)r * p];
           for (int r = 0; r < p; ++r)
             for (int c = r; c < p; ++c) {
               const cplx h = 0.5 * (Aj[r + (size_t)c * p] + std::conj(Aj[c + (size_t)r * p]));
@@ -715,20 +714,15 @@ static edk_status block_lanczos(int nops, edk_operator* const* ops,
     EDK_TRY_CUDA(cudaEventRecord(e0, st));
     EDK_RETURN_IF(spmm(V, W));
     EDK_TRY_CUDA(cudaEventRecord(e1, st));
-    // two classical block Gram-Schmidt passes against V_j and V_{j-1}
+    // one classical block Gram-Schmidt pass against V_j and V_{j-1}; the
+    // Cholesky-QR below runs twice
     EDK_RETURN_IF(gram(W, V, Q1.as<double2>()));
     if (j > 0) EDK_RETURN_IF(gram(W, U, Q2.as<double2>()));
     EDK_RETURN_IF(update(Q1.as<double2>(), V, W));
     if (j > 0) EDK_RETURN_IF(update(Q2.as<double2>(), U, W));
-    EDK_RETURN_IF(gram(W, V, Q1b.as<double2>()));
-    if (j > 0) EDK_RETURN_IF(gram(W, U, Q2b.as<double2>()));
-    EDK_RETURN_IF(update(Q1b.as<double2>(), V, W));
-    if (j > 0) EDK_RETURN_IF(update(Q2b.as<double2>(), U, W));
     EDK_RETURN_IF(cholqr(W, U));  // U (= V_{j-1}) is free now
     EDK_TRY_CUDA(cudaEventRecord(e2, st));
     EDK_TRY_CUDA(cudaMemcpyAsync(hA.data() + (size_t)j * nops * pp, Q1.p,
-                                 (size_t)nops * pp * sizeof(double2), cudaMemcpyDeviceToHost, st));
-    EDK_TRY_CUDA(cudaMemcpyAsync(hA2.data() + (size_t)j * nops * pp, Q1b.p,
                                  (size_t)nops * pp * sizeof(double2), cudaMemcpyDeviceToHost, st));
     EDK_TRY_CUDA(cudaMemcpyAsync(hB.data() + (size_t)(j + 1) * nops * pp, Bm.p,
                                  (size_t)nops * pp * sizeof(double2), cudaMemcpyDeviceToHost, st));
