@@ -192,8 +192,8 @@ edk_status edk_operator_materialize(edk_operator* op, int32_t enable, int64_t* e
 /* Block Lanczos over a batch of operators (e.g. the momentum sectors of one
  * chain), each with a block of `block` right-hand-side vectors: the block
  * form of EDKit's Lanczos recurrence (_lanczos_build!,
- * src/algorithms/TimeEvolution.jl:250-306) with two classical block
- * Gram-Schmidt passes against the two previous blocks and Cholesky-QR
+ * src/algorithms/TimeEvolution.jl:250-306) with one classical block
+ * Gram-Schmidt pass against the two previous blocks and Cholesky-QR
  * (twice) for the next block.  The lowest `nev` distinct eigenvalues of each
  * operator's block-tridiagonal matrix are returned in evals[q * nev + k]
  * (NaN where fewer exist).  x0: per operator a D_q x block column-major
