@@ -99,25 +99,33 @@ __global__ void __launch_bounds__(256) k_bapply_ff(const BOp* __restrict__ ops,
 template <int BK, class VT, int NN>
 __global__ void __launch_bounds__(256, plan_min_blocks<BK, VT>()) k_bapply_plan(const BOp* __restrict__ ops,
                                                      const int* __restrict__ tile2op,
+                                                     int64_t ntiles,
                                                      const VT* __restrict__ V, VT* __restrict__ wt,
                                                      const int* __restrict__ step,
                                                      const int* __restrict__ done) {
+  // a resident grid walks the tiles; the operator record and its tables are
+  // loaded into shared memory again only when the operator changes
   __shared__ FFTab<BK> sm;
   __shared__ __align__(16) BOp s_op;  // the operator record, read from shared memory
-  const int q = tile2op[blockIdx.x];
-  if (done[q]) return;
-  {
-    const int4* src = reinterpret_cast<const int4*>(ops + q);
-    int4* dst = reinterpret_cast<int4*>(&s_op);
-    for (int e = threadIdx.x; e < (int)(sizeof(BOp) / sizeof(int4)); e += blockDim.x) dst[e] = src[e];
-  }
-  __syncthreads();
-  const BOp& o = s_op;
-  ff_tab_fill<BK>(sm, o.b, o.op.plan.binom);
-  __syncthreads();
   const int j = *step;
-  plan_row<BK, VT, NN>(o.b, o.op, o.ff, sm, (blockIdx.x - o.tile0) * (int64_t)kTile + threadIdx.x,
-                   V + o.voff + (int64_t)j * o.D, wt + o.woff, 0);
+  int cur = -1;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int q = tile2op[tile];
+    if (done[q]) continue;
+    if (q != cur) {
+      __syncthreads();  // the previous operator's rows no longer read the tables
+      const int4* src = reinterpret_cast<const int4*>(ops + q);
+      int4* dst = reinterpret_cast<int4*>(&s_op);
+      for (int e = threadIdx.x; e < (int)(sizeof(BOp) / sizeof(int4)); e += blockDim.x) dst[e] = src[e];
+      __syncthreads();
+      ff_tab_fill<BK>(sm, s_op.b, s_op.op.plan.binom);
+      __syncthreads();
+      cur = q;
+    }
+    const BOp& o = s_op;
+    plan_row<BK, VT, NN>(o.b, o.op, o.ff, sm, (tile - o.tile0) * (int64_t)kTile + threadIdx.x,
+                         V + o.voff + (int64_t)j * o.D, wt + o.woff, 0);
+  }
 }
 
 template <class VT>
@@ -788,6 +796,7 @@ struct BatchEngine {
   std::vector<int64_t> Ds;
   int64_t ntiles = 0, totalD = 0;
   int G = 1;             // blocks of the reorthogonalisation grid
+  int nsm = 1;           // SMs of the device
   bool fused = false;    // first update and second dot products in one kernel
   DevBuf dops, tile2op, sblk2op, splitops, splitT, nfin, V, w, wt, part, coef1, coef2, normpart, alpha, beta, invb,
       done, step, nsteps, cbuf, cnc;
@@ -904,7 +913,7 @@ struct BatchEngine {
     }
     const size_t fs = us + (size_t)ncap * sizeof(double2);  // + column sums
     fused = fs <= 200 * 1024;
-    int dev = 0, nsm = 0;
+    int dev = 0;
     EDK_TRY_CUDA(cudaGetDevice(&dev));
     EDK_TRY_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     int per_sm = 0;
@@ -960,27 +969,35 @@ struct BatchEngine {
         switch (bk) {
           case BK_PROJ_RANK:
             if (plan_nn_all)
-              k_bapply_plan<BK_PROJ_RANK, VT, 1><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+              k_bapply_plan<BK_PROJ_RANK, VT, 1><<<plan_grid(plan_min_blocks<BK_PROJ_RANK, VT>()), 256, 0, st>>>(
+                  d_ops(), t2o, ntiles, Vv, wv, stp, dn);
             else
-              k_bapply_plan<BK_PROJ_RANK, VT, 2><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+              k_bapply_plan<BK_PROJ_RANK, VT, 2><<<plan_grid(plan_min_blocks<BK_PROJ_RANK, VT>()), 256, 0, st>>>(
+                  d_ops(), t2o, ntiles, Vv, wv, stp, dn);
             return EDK_OK;
           case BK_TRANS0_RANK:
             if (plan_nn_all)
-              k_bapply_plan<BK_TRANS0_RANK, VT, 1><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+              k_bapply_plan<BK_TRANS0_RANK, VT, 1><<<plan_grid(plan_min_blocks<BK_TRANS0_RANK, VT>()), 256, 0, st>>>(
+                  d_ops(), t2o, ntiles, Vv, wv, stp, dn);
             else
-              k_bapply_plan<BK_TRANS0_RANK, VT, 2><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+              k_bapply_plan<BK_TRANS0_RANK, VT, 2><<<plan_grid(plan_min_blocks<BK_TRANS0_RANK, VT>()), 256, 0, st>>>(
+                  d_ops(), t2o, ntiles, Vv, wv, stp, dn);
             return EDK_OK;
           case BK_TRANS_RANK:
             if (plan_nn_all)
-              k_bapply_plan<BK_TRANS_RANK, VT, 1><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+              k_bapply_plan<BK_TRANS_RANK, VT, 1><<<plan_grid(plan_min_blocks<BK_TRANS_RANK, VT>()), 256, 0, st>>>(
+                  d_ops(), t2o, ntiles, Vv, wv, stp, dn);
             else
-              k_bapply_plan<BK_TRANS_RANK, VT, 2><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+              k_bapply_plan<BK_TRANS_RANK, VT, 2><<<plan_grid(plan_min_blocks<BK_TRANS_RANK, VT>()), 256, 0, st>>>(
+                  d_ops(), t2o, ntiles, Vv, wv, stp, dn);
             return EDK_OK;
           case BK_TRANSPAR_RANK:
             if (plan_nn_all)
-              k_bapply_plan<BK_TRANSPAR_RANK, VT, 1><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+              k_bapply_plan<BK_TRANSPAR_RANK, VT, 1><<<plan_grid(plan_min_blocks<BK_TRANSPAR_RANK, VT>()), 256, 0, st>>>(
+                  d_ops(), t2o, ntiles, Vv, wv, stp, dn);
             else
-              k_bapply_plan<BK_TRANSPAR_RANK, VT, 2><<<(unsigned)ntiles, 256, 0, st>>>(d_ops(), t2o, Vv, wv, stp, dn);
+              k_bapply_plan<BK_TRANSPAR_RANK, VT, 2><<<plan_grid(plan_min_blocks<BK_TRANSPAR_RANK, VT>()), 256, 0, st>>>(
+                  d_ops(), t2o, ntiles, Vv, wv, stp, dn);
             return EDK_OK;
         }
       }
@@ -1015,6 +1032,12 @@ struct BatchEngine {
 #undef EDK_BAPPLY
       return EDK_OK;
     });
+  }
+
+  // resident grid of the row-plan matvec: per_sm blocks on every SM, at
+  // most one block per tile
+  unsigned plan_grid(int per_sm) const {
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)nsm * per_sm));
   }
 
   RowSplit rsplit() const {
